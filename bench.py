@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""bench.py -- ms per PRP-3 iteration at the 8M FFT on B200 (libowl, plain FP64 form).
+
+Workload (one "step" = one Gerbicz block of the reference's PRP loop,
+src/Gpu.cpp:1461-1483): modMul(check, data) then 1,000 squarings of data,
+for E = the seeded prime in [136M, 139M] (136,181,029) at N = 8M words
+(W = H = 2048, 16.2 bits/word). Inputs are resident in HBM when the timed region
+starts; the L2 is flushed (a 512 MiB write) between timed steps, outside the
+timing. After the timed region the res64 at every 1,000 iterations is compared
+with the GMP golden table and a full Gerbicz check (B extra squarings) is run.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's algorithm on the host cores: the reference's
+OpenCL kernels cannot run here, so its CPU restatement (oracle/ibdwt.c, all host
+threads) stands in, one 8M squaring per step. Multi-GPU runs are replicas (one
+exponent per GPU, no collective on the data path): value = max-over-ranks time /
+all iterations.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 20261203
+E_8M = 136181029      # oracle_seeded_prime(SEED + 2, 136M, 139M)
+W_8M, H_8M = 2048, 2048
+N_8M = 2 * W_8M * H_8M
+BLOCK = 1000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--block", type=int, default=BLOCK)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [x for x in sm if mx and x > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_golden(name):
+    path = os.path.join(ROOT, "tests", "golden", name + ".json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic_8m.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def cpu_port_ms_per_iter(E, N, iters, threads):
+    """The reference's IBDWT squaring restated on the CPU (oracle/ibdwt.c), ms per iteration."""
+    import ctypes
+    import numpy as np
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True,
+                   capture_output=True)
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    lib.oracle_ibdwt_create.restype = ctypes.c_void_p
+    lib.oracle_ibdwt_create.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int]
+    lib.oracle_ibdwt_square.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_int,
+                                        ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.oracle_ibdwt_destroy.argtypes = [ctypes.c_void_p]
+    lib.oracle_expand_bits.argtypes = [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.POINTER(ctypes.c_int32)]
+    p = lib.oracle_ibdwt_create(E, N, threads)
+    rng = np.random.default_rng(SEED)
+    nw = (E - 1) // 32 + 1
+    w = rng.integers(0, 2 ** 32, size=nw, dtype=np.uint64).astype(np.uint32)
+    if E % 32:
+        w[-1] &= (1 << (E % 32)) - 1
+    d = np.zeros(N, dtype=np.int32)
+    lib.oracle_expand_bits(w.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), N, E,
+                           d.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    roe = ctypes.c_double()
+    dp = d.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    lib.oracle_ibdwt_square(p, dp, 0, 0, ctypes.byref(roe))  # warm
+    times = []
+    for _ in range(iters):
+        t0 = time.perf_counter()
+        lib.oracle_ibdwt_square(p, dp, 0, 0, ctypes.byref(roe))
+        times.append(time.perf_counter() - t0)
+    lib.oracle_ibdwt_destroy(p)
+    return 1e3 * sum(times) / len(times), times
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    iters = args.warmup + args.steps
+    ms, _ = cpu_port_ms_per_iter(E_8M, N_8M, iters, threads)
+    line = {
+        "impl": "reference",
+        "metric": "ms/iter PRP @8M FFT: split-precision TC vs plain FP64, bit-exact res64",
+        "value": round(ms, 3), "unit": "ms/iter", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "PRP-3 squaring, E=136181029 (seeded prime in [136M,139M]), FFT 8M",
+                   "E": E_8M, "N": N_8M, "step": "one 8M IBDWT squaring on the host cores"},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms/iter", "cores": threads, "kind": "port",
+                         "sample": "%d squarings at E=%d, N=8M (oracle/ibdwt.c, OpenMP); the reference's "
+                                   "OpenCL kernels have no CPU runtime here" % (iters, E_8M)},
+        "e2e": {"value": round(ms, 3), "unit": "ms/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import gpuowl_b200 as owl
+    from gpuowl_b200 import build
+    build.build()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    B = args.block
+    plan = owl.Plan(E_8M, device=local, W=W_8M, H=H_8M)
+    stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", local))
+    data, check, aux = plan.alloc(), plan.alloc(), plan.alloc()
+    one = [1] + [0] * (plan.nwords - 1)
+    three = [3] + [0] * (plan.nwords - 1)
+    plan.writeIn(data, three)
+    plan.writeIn(check, one)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    golden = load_golden("prp_8m")
+    res = []
+
+    def step():
+        plan.modMul(check, data)
+        return plan.profile_square(data, B)
+
+    for _ in range(args.warmup):
+        step()
+        res.append("%016x" % plan.bufResidue(data))
+    plan.readROE()
+
+    step_ms, prof = [], {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p = step()
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            for k, (ms, n) in p.items():
+                prof[k][0] += ms
+                prof[k][1] += n
+            res.append("%016x" % plan.bufResidue(data))
+    torch.cuda.synchronize()
+    barrier()
+    total_ms = sum(step_ms)
+    roe = plan.readROE()
+
+    # Gerbicz check of the final state (reference doCheck, src/Gpu.cpp:767-771)
+    plan.squareLoop(aux, check, B, mul3=True)
+    plan.modMul(check, data)
+    gerbicz_ok = plan.isEqual(check, aux)
+
+    # e2e through the public API with host buffers: writeIn -> block -> readOut (+res64)
+    words = plan.readOut(data)
+    e2e_ms = []
+    barrier()
+    for _ in range(max(2, args.steps // 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plan.writeIn(data, words)
+        plan.modMul(check, data)
+        plan.squareLoop(data, data, B)
+        words = plan.readOut(data)
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    barrier()
+
+    if dist is not None:
+        t = torch.tensor([total_ms, sum(e2e_ms) / len(e2e_ms)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_step = float(t[0]), float(t[1])
+    else:
+        e2e_step = sum(e2e_ms) / len(e2e_ms)
+
+    iters_all = world * args.steps * B
+    value = total_ms / iters_all
+    n = min(len(res), len(golden["res64"])) if golden else 0
+    res_match = (res[:n] == golden["res64"][:n]) if golden else None
+
+    # roofline of the dominant kernel: algorithmic bytes per launch = read + write of the
+    # 8N-byte state = 16 N bytes, over its average launch time in the timed region
+    dom = "pass2" if prof["pass2"][0] >= prof["pass1"][0] else "pass1"
+    avg_ms = prof[dom][0] / max(prof[dom][1], 1)
+    alg_bytes = 16 * N_8M
+    achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic().get(dom)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        iters = 12
+        ms, _ = cpu_port_ms_per_iter(E_8M, N_8M, iters, os.cpu_count() or 1)
+        cpu = {"value": round(ms, 2), "unit": "ms/iter", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": "%d squarings at E=%d, N=8M with oracle/ibdwt.c (OpenMP, all host threads)"
+                         % (iters, E_8M)}
+
+    launches_per_step = 5 + 2 * B + 1
+    line = {
+        "metric": "ms/iter PRP @8M FFT: split-precision TC vs plain FP64, bit-exact res64",
+        "value": round(value, 5), "unit": "ms/iter", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "PRP-3, E=136181029 (seeded prime in [136M,139M]), FFT 8M (W=H=2048), "
+                               "plain FP64 form",
+                   "E": E_8M, "N": N_8M, "block": B, "step": "modMul(check,data) + %d squarings" % B,
+                   "timed_iterations": args.steps * B, "l2": "flushed (512 MiB write) between timed steps",
+                   "parallelism": "replicas x%d" % world},
+        "res64_match_golden": res_match, "res64_checked": n, "gerbicz_ok": bool(gerbicz_ok),
+        "max_roe": round(float(roe.max()), 5) if roe.size else None,
+        "kernel_ms": {k: round(v[0] / max(v[1], 1), 5) for k, v in prof.items()},
+        "roofline": {"bound": "hbm", "kernel": "k_pass2" if dom == "pass2" else "k_pass1",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e_step / B, 5), "unit": "ms/iter",
+                "h2d_bytes_per_step": 4 * N_8M, "d2h_bytes_per_step": 4 * N_8M + 8},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,243 @@
+"""gpuowl_b200 -- B200-native engine for the Mersenne PRP/LL squaring x <- x^2 (-2) mod 2^E-1.
+
+The engine is libowl.so (hand-written sm_100a CUDA behind the C ABI in
+include/owl.h). This module is a thin ctypes binding over that ABI, used by the
+tests and bench.py. There is no CPU path: importing works anywhere, but every
+operation needs libowl.so and a CUDA device, and raises OwlError otherwise.
+
+Names follow the reference's Gpu surface (src/Gpu.h): writeIn/readData,
+square/squareLoop, modMul, isEqual, bufResidue.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["OwlError", "load", "Plan", "n_words", "fft_choose", "LIB_PATH"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libowl.so")
+
+SQ_MUL3 = 1
+SQ_LL = 2
+
+OK = 0
+ERR_TIMEOUT = -4
+
+
+class OwlError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s (status %d)" % (msg, status))
+        self.status = status
+
+
+_lib = None
+
+_P = ctypes.c_void_p
+_I32P = ctypes.POINTER(ctypes.c_int32)
+_U32P = ctypes.POINTER(ctypes.c_uint32)
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+
+_SIGS = {
+    "owl_abi_version": ([], ctypes.c_int),
+    "owl_error_string": ([ctypes.c_int], ctypes.c_char_p),
+    "owl_last_error": ([], ctypes.c_char_p),
+    "owl_device_count": ([ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "owl_device_info": ([ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                         ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+    "owl_fft_choose": ([ctypes.c_uint32, ctypes.c_double, _U32P, _U32P, _U32P], ctypes.c_int),
+    "owl_plan_create": ([ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                         ctypes.POINTER(_P)], ctypes.c_int),
+    "owl_plan_destroy": ([_P], ctypes.c_int),
+    "owl_plan_shape": ([_P, _U32P, _U32P, _U32P], ctypes.c_int),
+    "owl_plan_set_timeout": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "owl_buf_alloc": ([_P, ctypes.POINTER(_P)], ctypes.c_int),
+    "owl_buf_free": ([_P, _P], ctypes.c_int),
+    "owl_buf_copy": ([_P, _P, _P], ctypes.c_int),
+    "owl_buf_set": ([_P, _P, ctypes.c_uint32], ctypes.c_int),
+    "owl_write_digits": ([_P, _P, _I32P], ctypes.c_int),
+    "owl_read_digits": ([_P, _P, _I32P], ctypes.c_int),
+    "owl_write_words": ([_P, _P, _U32P], ctypes.c_int),
+    "owl_read_words": ([_P, _P, _U32P], ctypes.c_int),
+    "owl_square": ([_P, _P, _P, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int),
+    "owl_modmul": ([_P, _P, _P, ctypes.c_int], ctypes.c_int),
+    "owl_is_equal": ([_P, _P, _P, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "owl_res64": ([_P, _P, _U64P], ctypes.c_int),
+    "owl_sum64": ([_P, _P, _U64P], ctypes.c_int),
+    "owl_read_roe": ([_P, ctypes.POINTER(ctypes.c_float), ctypes.c_uint32, _U32P], ctypes.c_int),
+    "owl_sync": ([_P], ctypes.c_int),
+    "owl_probe_wait_timeout": ([_P], ctypes.c_int),
+    "owl_plan_stream": ([_P, ctypes.POINTER(_P)], ctypes.c_int),
+    "owl_profile_square": ([_P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), _U32P], ctypes.c_int),
+}
+
+
+def load(path=None):
+    """Load libowl.so (built by gpuowl_b200/build.py). Raises OwlError if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise OwlError(-100, "libowl.so not built (run python -m gpuowl_b200.build): " + p)
+    lib = ctypes.CDLL(p)
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    if lib.owl_abi_version() != 1:
+        raise OwlError(-100, "libowl ABI mismatch")
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(status):
+    if status != OK:
+        lib = load()
+        raise OwlError(status, lib.owl_last_error().decode(errors="replace") or
+                       lib.owl_error_string(status).decode())
+
+
+def n_words(E):
+    """(E-1)/32+1 compact u32 words (reference src/common.h nWords)."""
+    return (E - 1) // 32 + 1
+
+
+def fft_choose(E, max_bpw=0.0):
+    lib = load()
+    N, W, H = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    _check(lib.owl_fft_choose(E, max_bpw, ctypes.byref(N), ctypes.byref(W), ctypes.byref(H)))
+    return N.value, W.value, H.value
+
+
+def device_count():
+    lib = load()
+    n = ctypes.c_int(0)
+    _check(lib.owl_device_count(ctypes.byref(n)))
+    return n.value
+
+
+class Plan:
+    """One exponent on one device (reference Gpu, src/Gpu.cpp:394-564).
+
+    Word buffers are device pointers (ints) returned by alloc(); they hold N
+    balanced int32 digits in natural word order.
+    """
+
+    def __init__(self, E, device=0, W=0, H=0):
+        self.lib = load()
+        self.E = int(E)
+        self.device = device
+        h = _P()
+        _check(self.lib.owl_plan_create(device, self.E, W, H, ctypes.byref(h)))
+        self.h = h
+        N, Wv, Hv = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(self.lib.owl_plan_shape(self.h, ctypes.byref(N), ctypes.byref(Wv), ctypes.byref(Hv)))
+        self.N, self.W, self.H = N.value, Wv.value, Hv.value
+        self.nwords = n_words(self.E)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _check(self.lib.owl_plan_destroy(self.h))
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- buffers --
+    def alloc(self):
+        b = _P()
+        _check(self.lib.owl_buf_alloc(self.h, ctypes.byref(b)))
+        return b.value
+
+    def free(self, buf):
+        _check(self.lib.owl_buf_free(self.h, buf))
+
+    def copy(self, dst, src):
+        _check(self.lib.owl_buf_copy(self.h, dst, src))
+
+    def set(self, buf, value):
+        _check(self.lib.owl_buf_set(self.h, buf, value))
+
+    def set_timeout(self, ns):
+        _check(self.lib.owl_plan_set_timeout(self.h, int(ns)))
+
+    def write_digits(self, buf, digits):
+        d = np.ascontiguousarray(digits, dtype=np.int32)
+        assert d.size == self.N
+        _check(self.lib.owl_write_digits(self.h, buf, d.ctypes.data_as(_I32P)))
+
+    def read_digits(self, buf):
+        d = np.empty(self.N, dtype=np.int32)
+        _check(self.lib.owl_read_digits(self.h, buf, d.ctypes.data_as(_I32P)))
+        return d
+
+    def writeIn(self, buf, words):
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        assert w.size == self.nwords
+        _check(self.lib.owl_write_words(self.h, buf, w.ctypes.data_as(_U32P)))
+
+    def readOut(self, buf):
+        """Compact words of a buffer (reference readAndCompress: checked read + compactBits)."""
+        w = np.empty(self.nwords, dtype=np.uint32)
+        _check(self.lib.owl_read_words(self.h, buf, w.ctypes.data_as(_U32P)))
+        return w
+
+    # -- engine ops --
+    def squareLoop(self, out, inp, n, mul3=False, ll=False):
+        flags = (SQ_MUL3 if mul3 else 0) | (SQ_LL if ll else 0)
+        _check(self.lib.owl_square(self.h, out, inp, int(n), flags))
+
+    def modMul(self, io_a, in_b, mul3=False):
+        _check(self.lib.owl_modmul(self.h, io_a, in_b, 1 if mul3 else 0))
+
+    def isEqual(self, a, b):
+        r = ctypes.c_int(0)
+        _check(self.lib.owl_is_equal(self.h, a, b, ctypes.byref(r)))
+        return bool(r.value)
+
+    def bufResidue(self, buf):
+        r = ctypes.c_uint64(0)
+        _check(self.lib.owl_res64(self.h, buf, ctypes.byref(r)))
+        return r.value
+
+    def sum64(self, buf):
+        r = ctypes.c_uint64(0)
+        _check(self.lib.owl_sum64(self.h, buf, ctypes.byref(r)))
+        return r.value
+
+    def readROE(self, cap=1 << 16):
+        arr = (ctypes.c_float * cap)()
+        n = ctypes.c_uint32(0)
+        _check(self.lib.owl_read_roe(self.h, arr, cap, ctypes.byref(n)))
+        return np.array(arr[:n.value], dtype=np.float32)
+
+    def sync(self):
+        _check(self.lib.owl_sync(self.h))
+
+    def stream(self):
+        """The plan's cudaStream_t as an int (wrap with torch.cuda.ExternalStream)."""
+        s = _P()
+        _check(self.lib.owl_plan_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def profile_square(self, buf, n):
+        """Per-kernel device time of n squarings: {"pass2": (ms, launches), "pass1": ..., "edge": ...}."""
+        ms = (ctypes.c_float * 3)()
+        cnt = (ctypes.c_uint32 * 3)()
+        _check(self.lib.owl_profile_square(self.h, buf, int(n), ms, cnt))
+        return {"pass2": (ms[0], cnt[0]), "pass1": (ms[1], cnt[1]), "edge": (ms[2], cnt[2])}
+
+    def probe_wait_timeout(self):
+        """Returns the status of a device wait that must time out (ERR_TIMEOUT)."""
+        return self.lib.owl_probe_wait_timeout(self.h)

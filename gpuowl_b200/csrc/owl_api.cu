@@ -1,0 +1,742 @@
+// owl_api.cu -- libowl: plans, buffers and the C ABI of include/owl.h.
+//
+// Per squaring the engine launches two kernels (k_pass2 then k_pass1), the
+// B200 counterpart of the reference's four-kernel chain fftMiddleIn ->
+// tailSquare -> fftMiddleOut -> carryFused (src/Gpu.cpp:851-856, 903-932).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "owl.h"
+#include "owl_kernels.cuh"
+#include "owl_tables.hpp"
+#include "owl_words.hpp"
+
+using owl::C;
+
+namespace {
+
+thread_local std::string g_lastError;
+
+struct OwlError {
+  int code;
+  std::string msg;
+};
+
+void fail(int code, const std::string& msg) { throw OwlError{code, msg}; }
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    fail(e == cudaErrorMemoryAllocation ? OWL_ERR_NOMEM : OWL_ERR_CUDA,
+         std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+template <typename F> int guarded(F&& f) {
+  try {
+    f();
+    return OWL_OK;
+  } catch (const OwlError& e) {
+    g_lastError = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_lastError = "host allocation failed";
+    return OWL_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    g_lastError = e.what();
+    return OWL_ERR_ARG;
+  }
+}
+
+constexpr int kR = 2;                    // lines per pass-1 CTA
+constexpr uint32_t kRoeCap = 1u << 16;   // per-launch ROE slots
+constexpr double kDefaultMaxBpw = 19.2;  // at N = 256K; lowered 0.3 per doubling
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) { ck(cudaSetDevice(dev), "cudaSetDevice"); }
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) { cudaSetDevice(prev); }
+  }
+};
+
+}  // namespace
+
+struct owl_plan {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t E = 0, N = 0, W = 0, H = 0, hN = 0;
+  owl::Args args{};
+  C* F1 = nullptr;
+  C* F2 = nullptr;
+  void* tableMem = nullptr;
+  void* scratch = nullptr;  // shuttle, flags, ctl, roe, small outputs
+  int32_t* small = nullptr; // 64 gathered words
+  unsigned long long* sum = nullptr;
+  int* eq = nullptr;
+  uint32_t roePos = 0;
+  std::vector<int32_t*> bufs;
+};
+
+namespace {
+
+// ---- kernel dispatch on the compile-time shape --------------------------------
+
+template <int W, int M> void setp1attr() {
+  size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
+  ck(cudaFuncSetAttribute(owl::k_pass1<W, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+     "cudaFuncSetAttribute(pass1)");
+}
+template <int H, int M> void setp2attr() {
+  size_t sm = 2 * (size_t)owl::p2_col_stride<H>() * sizeof(C);
+  ck(cudaFuncSetAttribute(owl::k_pass2<H, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+     "cudaFuncSetAttribute(pass2)");
+}
+
+template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags) {
+  constexpr int T = kR * W / 16;
+  size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
+  dim3 grid(p->H / kR);
+  switch (mode) {
+    case owl::P1_FUSED:
+      owl::k_pass1<W, kR, owl::P1_FUSED><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags);
+      break;
+    case owl::P1_IN:
+      owl::k_pass1<W, kR, owl::P1_IN><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags);
+      break;
+    default:
+      owl::k_pass1<W, kR, owl::P1_OUT><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags);
+      break;
+  }
+}
+
+template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq) {
+  constexpr int T = H / 8;
+  size_t sm = 2 * (size_t)owl::p2_col_stride<H>() * sizeof(C);
+  dim3 grid(p->W / 2);
+  switch (mode) {
+    case owl::P2_SQUARE:
+      owl::k_pass2<H, kR, owl::P2_SQUARE><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq);
+      break;
+    case owl::P2_FWD:
+      owl::k_pass2<H, kR, owl::P2_FWD><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq);
+      break;
+    default:
+      owl::k_pass2<H, kR, owl::P2_MUL><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq);
+      break;
+  }
+}
+
+#define OWL_FOR_SIZES(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+
+void set_attrs(uint32_t W, uint32_t H) {
+  switch (W) {
+#define CASE_W(n)                  \
+  case n:                          \
+    setp1attr<n, owl::P1_FUSED>(); \
+    setp1attr<n, owl::P1_IN>();    \
+    setp1attr<n, owl::P1_OUT>();   \
+    break;
+    OWL_FOR_SIZES(CASE_W)
+#undef CASE_W
+    default:
+      fail(OWL_ERR_ARG, "unsupported W");
+  }
+  switch (H) {
+#define CASE_H(n)                   \
+  case n:                           \
+    setp2attr<n, owl::P2_SQUARE>(); \
+    setp2attr<n, owl::P2_FWD>();    \
+    setp2attr<n, owl::P2_MUL>();    \
+    break;
+    OWL_FOR_SIZES(CASE_H)
+#undef CASE_H
+    default:
+      fail(OWL_ERR_ARG, "unsupported H");
+  }
+}
+
+void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags) {
+  int slot = -1;
+  if (mode != owl::P1_IN) {
+    slot = (int)std::min(p->roePos, kRoeCap - 1);
+    if (p->roePos < kRoeCap) { ++p->roePos; }
+  }
+  switch (p->W) {
+#define CASE_W(n)                                \
+  case n:                                        \
+    p1launch<n>(p, mode, F, words, slot, flags); \
+    break;
+    OWL_FOR_SIZES(CASE_W)
+#undef CASE_W
+    default:
+      fail(OWL_ERR_ARG, "unsupported W");
+  }
+  ck(cudaGetLastError(), "pass1 launch");
+}
+
+void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq) {
+  switch (p->H) {
+#define CASE_H(n)                       \
+  case n:                               \
+    p2launch<n>(p, mode, F, Fb, Fq);    \
+    break;
+    OWL_FOR_SIZES(CASE_H)
+#undef CASE_H
+    default:
+      fail(OWL_ERR_ARG, "unsupported H");
+  }
+  ck(cudaGetLastError(), "pass2 launch");
+}
+
+void check_plan(const owl_plan* p) {
+  if (!p) { fail(OWL_ERR_ARG, "null plan"); }
+}
+
+void check_buf(const owl_plan* p, const int32_t* b) {
+  if (!b) { fail(OWL_ERR_ARG, "null buffer"); }
+  if (std::find(p->bufs.begin(), p->bufs.end(), b) == p->bufs.end()) {
+    fail(OWL_ERR_ARG, "buffer does not belong to this plan");
+  }
+}
+
+// reads and clears the device error word; throws on a recorded wait timeout
+void sync_and_check(owl_plan* p) {
+  ck(cudaStreamSynchronize(p->stream), "cudaStreamSynchronize");
+  uint32_t err = 0;
+  ck(cudaMemcpy(&err, &p->args.ctl->error, sizeof(err), cudaMemcpyDeviceToHost), "read error word");
+  if (err) {
+    // reset the carry-chain state so that the plan stays usable
+    uint32_t G = p->H / kR;
+    ck(cudaMemset(p->args.ctl, 0, sizeof(owl::Ctl)), "reset ctl");
+    ck(cudaMemset(p->args.flags, 0, G * sizeof(uint32_t)), "reset flags");
+    fail(OWL_ERR_TIMEOUT, "device-side carry wait timed out");
+  }
+}
+
+template <typename T> T* carve(char*& cur, size_t count) {
+  size_t off = (reinterpret_cast<uintptr_t>(cur) + 255) & ~uintptr_t(255);
+  T* r = reinterpret_cast<T*>(off);
+  cur = reinterpret_cast<char*>(off + count * sizeof(T));
+  return r;
+}
+
+void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out) {
+  if (!out) { fail(OWL_ERR_ARG, "null out"); }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    fail(OWL_ERR_NODEV, "no CUDA device " + std::to_string(device));
+  }
+  if (E < 1000 || E % 2 == 0) { fail(OWL_ERR_ARG, "exponent must be odd and >= 1000"); }
+  if (W == 0 && H == 0) {
+    uint32_t N;
+    if (owl_fft_choose(E, 0, &N, &W, &H) != OWL_OK) { fail(OWL_ERR_ARG, "no FFT shape for this exponent"); }
+  }
+  if (!owl::is_pow2(W) || !owl::is_pow2(H) || W < 64 || W > 4096 || H < 64 || H > 4096) {
+    fail(OWL_ERR_ARG, "W and H must be powers of two in [64, 4096]");
+  }
+  const uint32_t N = 2 * W * H;
+  // below ~8 bits per word the sloppy carry-in of a line group can overflow a
+  // digit; above ~21 the FP64 round-off can reach 0.5 at any size built here
+  if (E / N < 8 || (double)E / N > 21.0) { fail(OWL_ERR_ARG, "bits per word out of range for this FFT"); }
+
+  owl::Tables t = owl::make_tables(E, W, H);
+
+  DeviceGuard dg(device);
+  std::unique_ptr<owl_plan> p(new owl_plan());
+  p->device = device;
+  p->E = E;
+  p->N = N;
+  p->W = W;
+  p->H = H;
+  p->hN = W * H;
+  set_attrs(W, H);
+  ck(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+
+  // tables: one allocation
+  size_t nC = t.twW.size() + t.twH.size() + t.twLo.size() + t.twHi.size();
+  size_t bytes = 256 * 12 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
+                 (t.x1.size() + t.x2.size()) * sizeof(uint32_t);
+  ck(cudaMalloc(&p->tableMem, bytes), "cudaMalloc(tables)");
+  std::vector<char> host(bytes, 0);
+  char* hcur = host.data();
+  auto put = [&](const void* src, size_t n) -> size_t {
+    size_t off = ((size_t)(hcur - host.data()) + 255) & ~size_t(255);
+    std::memcpy(host.data() + off, src, n);
+    hcur = host.data() + off + n;
+    return off;
+  };
+  char* dbase = static_cast<char*>(p->tableMem);
+  p->args.twW = reinterpret_cast<const C*>(dbase + put(t.twW.data(), t.twW.size() * sizeof(C)));
+  p->args.twH = reinterpret_cast<const C*>(dbase + put(t.twH.data(), t.twH.size() * sizeof(C)));
+  p->args.twLo = reinterpret_cast<const C*>(dbase + put(t.twLo.data(), t.twLo.size() * sizeof(C)));
+  p->args.twHi = reinterpret_cast<const C*>(dbase + put(t.twHi.data(), t.twHi.size() * sizeof(C)));
+  p->args.wt1 = reinterpret_cast<const double*>(dbase + put(t.wt1.data(), t.wt1.size() * sizeof(double)));
+  p->args.iwt1 = reinterpret_cast<const double*>(dbase + put(t.iwt1.data(), t.iwt1.size() * sizeof(double)));
+  p->args.x1 = reinterpret_cast<const uint32_t*>(dbase + put(t.x1.data(), t.x1.size() * sizeof(uint32_t)));
+  p->args.wt2 = reinterpret_cast<const double*>(dbase + put(t.wt2.data(), t.wt2.size() * sizeof(double)));
+  p->args.iwt2 = reinterpret_cast<const double*>(dbase + put(t.iwt2.data(), t.iwt2.size() * sizeof(double)));
+  p->args.x2 = reinterpret_cast<const uint32_t*>(dbase + put(t.x2.data(), t.x2.size() * sizeof(uint32_t)));
+  ck(cudaMemcpy(p->tableMem, host.data(), bytes, cudaMemcpyHostToDevice), "upload tables");
+
+  // FFT work buffers
+  ck(cudaMalloc(&p->F1, (size_t)p->hN * sizeof(C)), "cudaMalloc(F1)");
+  ck(cudaMalloc(&p->F2, (size_t)p->hN * sizeof(C)), "cudaMalloc(F2)");
+
+  // scratch: carry shuttle, flags, control word, ROE slots, small outputs
+  const uint32_t G = H / kR;
+  size_t sbytes = 256 * 8 + (size_t)G * W * sizeof(long long) + G * sizeof(uint32_t) + sizeof(owl::Ctl) +
+                  kRoeCap * sizeof(float) + 64 * sizeof(int32_t) + sizeof(unsigned long long) + sizeof(int);
+  ck(cudaMalloc(&p->scratch, sbytes), "cudaMalloc(scratch)");
+  ck(cudaMemset(p->scratch, 0, sbytes), "memset(scratch)");
+  char* cur = static_cast<char*>(p->scratch);
+  p->args.shuttle = carve<long long>(cur, (size_t)G * W);
+  p->args.flags = carve<uint32_t>(cur, G);
+  p->args.ctl = carve<owl::Ctl>(cur, 1);
+  p->args.roe = carve<float>(cur, kRoeCap);
+  p->small = carve<int32_t>(cur, 64);
+  p->sum = carve<unsigned long long>(cur, 1);
+  p->eq = carve<int>(cur, 1);
+
+  p->args.E = E;
+  p->args.N = N;
+  p->args.W = W;
+  p->args.H = H;
+  p->args.hN = p->hN;
+  p->args.bitsLo = E / N;
+  p->args.eModN = E % N;
+  p->args.loShift = t.loShift;
+  p->args.timeoutNs = 2000000000ull;
+  *out = p.release();
+}
+
+void plan_destroy(owl_plan* p) {
+  DeviceGuard dg(p->device);
+  if (p->stream) { cudaStreamSynchronize(p->stream); }
+  for (int32_t* b : p->bufs) { cudaFree(b); }
+  cudaFree(p->F1);
+  cudaFree(p->F2);
+  cudaFree(p->tableMem);
+  cudaFree(p->scratch);
+  if (p->stream) { cudaStreamDestroy(p->stream); }
+  delete p;
+}
+
+void checked_download(owl_plan* p, const int32_t* buf, std::vector<int32_t>& host) {
+  host.resize(p->N);
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    ck(cudaMemsetAsync(p->sum, 0, sizeof(unsigned long long), p->stream), "memset sum");
+    owl::k_sum64<<<296, 256, 0, p->stream>>>(reinterpret_cast<const unsigned long long*>(buf), p->N / 2, p->sum);
+    ck(cudaGetLastError(), "sum64 launch");
+    unsigned long long gpuSum = 0;
+    ck(cudaMemcpyAsync(&gpuSum, p->sum, sizeof(gpuSum), cudaMemcpyDeviceToHost, p->stream), "read sum");
+    ck(cudaMemcpyAsync(host.data(), buf, (size_t)p->N * sizeof(int32_t), cudaMemcpyDeviceToHost, p->stream),
+       "read words");
+    sync_and_check(p);
+    unsigned long long hostSum = 0;
+    for (uint32_t i = 0; i + 1 < p->N; i += 2) {
+      hostSum += (uint64_t)(uint32_t)host[i] | ((uint64_t)(uint32_t)host[i + 1] << 32);
+    }
+    if (hostSum == gpuSum) { return; }
+  }
+  fail(OWL_ERR_READ, "GPU persistent read errors");
+}
+
+}  // namespace
+
+extern "C" {
+
+int owl_abi_version(void) { return OWL_ABI_VERSION; }
+
+const char* owl_error_string(int status) {
+  switch (status) {
+    case OWL_OK: return "ok";
+    case OWL_ERR_ARG: return "bad argument";
+    case OWL_ERR_NOMEM: return "out of memory";
+    case OWL_ERR_CUDA: return "CUDA error";
+    case OWL_ERR_TIMEOUT: return "device wait timeout";
+    case OWL_ERR_NODEV: return "no such device";
+    case OWL_ERR_READ: return "persistent read errors";
+    default: return "unknown status";
+  }
+}
+
+const char* owl_last_error(void) { return g_lastError.c_str(); }
+
+int owl_device_count(int* count) {
+  return guarded([&] {
+    if (!count) { fail(OWL_ERR_ARG, "null count"); }
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    *count = (e == cudaSuccess) ? n : 0;
+  });
+}
+
+int owl_device_info(int ordinal, char* name, size_t name_len, size_t* total_mem, char* pci, size_t pci_len) {
+  return guarded([&] {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ordinal) != cudaSuccess) { fail(OWL_ERR_NODEV, "no such device"); }
+    if (name && name_len) { std::snprintf(name, name_len, "%s", prop.name); }
+    if (total_mem) { *total_mem = prop.totalGlobalMem; }
+    if (pci && pci_len) { ck(cudaDeviceGetPCIBusId(pci, (int)pci_len, ordinal), "cudaDeviceGetPCIBusId"); }
+  });
+}
+
+int owl_fft_choose(uint32_t E, double max_bpw, uint32_t* N, uint32_t* W, uint32_t* H) {
+  return guarded([&] {
+    if (!N || !W || !H) { fail(OWL_ERR_ARG, "null output"); }
+    for (uint32_t lg = 13; lg <= 25; ++lg) {
+      uint32_t n = 1u << lg;
+      double lim = max_bpw > 0 ? max_bpw : kDefaultMaxBpw - 0.3 * ((double)lg - 18.0);
+      if ((double)E / n > lim) { continue; }
+      uint32_t w = 1u << ((lg - 1) / 2);
+      uint32_t h = (n / 2) / w;
+      if (w < 64 || h > 4096) { break; }
+      *N = n;
+      *W = w;
+      *H = h;
+      return;
+    }
+    fail(OWL_ERR_ARG, "exponent outside the supported FFT range");
+  });
+}
+
+int owl_plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out) {
+  return guarded([&] { plan_create(device, E, W, H, out); });
+}
+
+int owl_plan_destroy(owl_plan* plan) {
+  return guarded([&] {
+    check_plan(plan);
+    plan_destroy(plan);
+  });
+}
+
+int owl_plan_shape(const owl_plan* plan, uint32_t* N, uint32_t* W, uint32_t* H) {
+  return guarded([&] {
+    check_plan(plan);
+    if (N) { *N = plan->N; }
+    if (W) { *W = plan->W; }
+    if (H) { *H = plan->H; }
+  });
+}
+
+int owl_plan_set_timeout(owl_plan* plan, uint64_t ns) {
+  return guarded([&] {
+    check_plan(plan);
+    if (ns == 0) { fail(OWL_ERR_ARG, "timeout must be positive"); }
+    plan->args.timeoutNs = ns;
+  });
+}
+
+int owl_buf_alloc(owl_plan* plan, int32_t** buf) {
+  return guarded([&] {
+    check_plan(plan);
+    if (!buf) { fail(OWL_ERR_ARG, "null out"); }
+    DeviceGuard dg(plan->device);
+    int32_t* b = nullptr;
+    ck(cudaMalloc(&b, (size_t)plan->N * sizeof(int32_t)), "cudaMalloc(words)");
+    cudaError_t e = cudaMemsetAsync(b, 0, (size_t)plan->N * sizeof(int32_t), plan->stream);
+    if (e != cudaSuccess) {
+      cudaFree(b);
+      ck(e, "memset(words)");
+    }
+    plan->bufs.push_back(b);
+    *buf = b;
+  });
+}
+
+int owl_buf_free(owl_plan* plan, int32_t* buf) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    DeviceGuard dg(plan->device);
+    ck(cudaStreamSynchronize(plan->stream), "sync");
+    plan->bufs.erase(std::find(plan->bufs.begin(), plan->bufs.end(), buf));
+    ck(cudaFree(buf), "cudaFree");
+  });
+}
+
+int owl_buf_copy(owl_plan* plan, int32_t* dst, const int32_t* src) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, dst);
+    check_buf(plan, src);
+    DeviceGuard dg(plan->device);
+    ck(cudaMemcpyAsync(dst, src, (size_t)plan->N * sizeof(int32_t), cudaMemcpyDeviceToDevice, plan->stream),
+       "copy");
+  });
+}
+
+int owl_buf_set(owl_plan* plan, int32_t* buf, uint32_t value) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    std::vector<uint32_t> w(owl::n_words(plan->E), 0);
+    w[0] = value;
+    std::vector<int32_t> d(plan->N);
+    if (!owl::expand_bits(w.data(), plan->N, plan->E, d.data())) { fail(OWL_ERR_ARG, "expand failed"); }
+    DeviceGuard dg(plan->device);
+    ck(cudaMemcpyAsync(buf, d.data(), (size_t)plan->N * sizeof(int32_t), cudaMemcpyHostToDevice, plan->stream),
+       "upload");
+    ck(cudaStreamSynchronize(plan->stream), "sync");
+  });
+}
+
+int owl_write_digits(owl_plan* plan, int32_t* buf, const int32_t* host) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    if (!host) { fail(OWL_ERR_ARG, "null host"); }
+    DeviceGuard dg(plan->device);
+    ck(cudaMemcpyAsync(buf, host, (size_t)plan->N * sizeof(int32_t), cudaMemcpyHostToDevice, plan->stream),
+       "upload");
+    ck(cudaStreamSynchronize(plan->stream), "sync");
+  });
+}
+
+int owl_read_digits(owl_plan* plan, const int32_t* buf, int32_t* host) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    if (!host) { fail(OWL_ERR_ARG, "null host"); }
+    DeviceGuard dg(plan->device);
+    ck(cudaMemcpyAsync(host, buf, (size_t)plan->N * sizeof(int32_t), cudaMemcpyDeviceToHost, plan->stream),
+       "download");
+    sync_and_check(plan);
+  });
+}
+
+int owl_write_words(owl_plan* plan, int32_t* buf, const uint32_t* words) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    if (!words) { fail(OWL_ERR_ARG, "null words"); }
+    std::vector<int32_t> d(plan->N);
+    if (!owl::expand_bits(words, plan->N, plan->E, d.data())) { fail(OWL_ERR_ARG, "expandBits failed"); }
+    DeviceGuard dg(plan->device);
+    ck(cudaMemcpyAsync(buf, d.data(), (size_t)plan->N * sizeof(int32_t), cudaMemcpyHostToDevice, plan->stream),
+       "upload");
+    ck(cudaStreamSynchronize(plan->stream), "sync");
+  });
+}
+
+int owl_read_words(owl_plan* plan, const int32_t* buf, uint32_t* words) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    if (!words) { fail(OWL_ERR_ARG, "null words"); }
+    DeviceGuard dg(plan->device);
+    std::vector<int32_t> d;
+    checked_download(plan, buf, d);
+    if (!owl::compact_bits(d.data(), plan->N, plan->E, words)) { fail(OWL_ERR_READ, "digit out of range"); }
+  });
+}
+
+int owl_square(owl_plan* plan, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, out);
+    check_buf(plan, in);
+    if (n == 0) {
+      if (out != in) { owl_buf_copy(plan, out, in); }
+      return;
+    }
+    DeviceGuard dg(plan->device);
+    const int ll = (flags & OWL_SQ_LL) ? owl::FL_LL : 0;
+    const int mul3 = (flags & OWL_SQ_MUL3) ? owl::FL_MUL3 : 0;
+    pass1(plan, owl::P1_IN, plan->F1, const_cast<int32_t*>(in), 0);
+    for (uint32_t k = 0; k < n; ++k) {
+      pass2(plan, owl::P2_SQUARE, plan->F1, nullptr, nullptr);
+      if (k + 1 < n) {
+        pass1(plan, owl::P1_FUSED, plan->F1, nullptr, ll);
+      } else {
+        pass1(plan, owl::P1_OUT, plan->F1, out, ll | mul3);
+      }
+    }
+  });
+}
+
+int owl_modmul(owl_plan* plan, int32_t* io_a, const int32_t* in_b, int mul3) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, io_a);
+    check_buf(plan, in_b);
+    DeviceGuard dg(plan->device);
+    pass1(plan, owl::P1_IN, plan->F2, const_cast<int32_t*>(in_b), 0);
+    pass2(plan, owl::P2_FWD, plan->F2, nullptr, plan->F2);
+    pass1(plan, owl::P1_IN, plan->F1, io_a, 0);
+    pass2(plan, owl::P2_MUL, plan->F1, plan->F2, nullptr);
+    pass1(plan, owl::P1_OUT, plan->F1, io_a, mul3 ? owl::FL_MUL3 : 0);
+  });
+}
+
+int owl_is_equal(owl_plan* plan, const int32_t* a, const int32_t* b, int* equal) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, a);
+    check_buf(plan, b);
+    if (!equal) { fail(OWL_ERR_ARG, "null out"); }
+    DeviceGuard dg(plan->device);
+    int one = 1;
+    ck(cudaMemcpyAsync(plan->eq, &one, sizeof(int), cudaMemcpyHostToDevice, plan->stream), "set eq");
+    owl::k_is_equal<<<296, 256, 0, plan->stream>>>(a, b, plan->N, plan->eq);
+    ck(cudaGetLastError(), "isEqual launch");
+    int r = 0;
+    ck(cudaMemcpyAsync(&r, plan->eq, sizeof(int), cudaMemcpyDeviceToHost, plan->stream), "read eq");
+    sync_and_check(plan);
+    *equal = r;
+  });
+}
+
+int owl_res64(owl_plan* plan, const int32_t* buf, uint64_t* res64) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    if (!res64) { fail(OWL_ERR_ARG, "null out"); }
+    DeviceGuard dg(plan->device);
+    owl::k_gather_residue<<<1, 64, 0, plan->stream>>>(buf, plan->N, plan->small);
+    ck(cudaGetLastError(), "gather launch");
+    int32_t w[64];
+    ck(cudaMemcpyAsync(w, plan->small, sizeof(w), cudaMemcpyDeviceToHost, plan->stream), "read residue words");
+    sync_and_check(plan);
+    bool decided = false;
+    uint64_t r = owl::residue_from_wrap(w, plan->N, plan->E, &decided);
+    if (!decided) {
+      std::vector<int32_t> d;
+      checked_download(plan, buf, d);
+      std::vector<uint32_t> words(owl::n_words(plan->E));
+      if (!owl::compact_bits(d.data(), plan->N, plan->E, words.data())) { fail(OWL_ERR_READ, "digit out of range"); }
+      r = (uint64_t)words[0] | ((words.size() > 1 ? (uint64_t)words[1] : 0) << 32);
+    }
+    *res64 = r;
+  });
+}
+
+int owl_sum64(owl_plan* plan, const int32_t* buf, uint64_t* sum) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    if (!sum) { fail(OWL_ERR_ARG, "null out"); }
+    DeviceGuard dg(plan->device);
+    ck(cudaMemsetAsync(plan->sum, 0, sizeof(unsigned long long), plan->stream), "memset sum");
+    owl::k_sum64<<<296, 256, 0, plan->stream>>>(reinterpret_cast<const unsigned long long*>(buf), plan->N / 2,
+                                                 plan->sum);
+    ck(cudaGetLastError(), "sum64 launch");
+    unsigned long long s = 0;
+    ck(cudaMemcpyAsync(&s, plan->sum, sizeof(s), cudaMemcpyDeviceToHost, plan->stream), "read sum");
+    sync_and_check(plan);
+    *sum = s;
+  });
+}
+
+int owl_read_roe(owl_plan* plan, float* out, uint32_t cap, uint32_t* n) {
+  return guarded([&] {
+    check_plan(plan);
+    if (!n) { fail(OWL_ERR_ARG, "null out"); }
+    DeviceGuard dg(plan->device);
+    uint32_t cnt = plan->roePos;
+    std::vector<float> host(cnt);
+    if (cnt) {
+      ck(cudaMemcpyAsync(host.data(), plan->args.roe, cnt * sizeof(float), cudaMemcpyDeviceToHost, plan->stream),
+         "read roe");
+      ck(cudaMemsetAsync(plan->args.roe, 0, cnt * sizeof(float), plan->stream), "clear roe");
+    }
+    sync_and_check(plan);
+    plan->roePos = 0;
+    uint32_t m = std::min(cnt, cap);
+    if (out && m) { std::memcpy(out, host.data(), m * sizeof(float)); }
+    *n = out ? m : cnt;
+  });
+}
+
+int owl_sync(owl_plan* plan) {
+  return guarded([&] {
+    check_plan(plan);
+    DeviceGuard dg(plan->device);
+    sync_and_check(plan);
+  });
+}
+
+int owl_plan_stream(owl_plan* plan, void** stream) {
+  return guarded([&] {
+    check_plan(plan);
+    if (!stream) { fail(OWL_ERR_ARG, "null out"); }
+    *stream = (void*)plan->stream;
+  });
+}
+
+int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint32_t* launches) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, buf);
+    if (!ms || !launches || n == 0) { fail(OWL_ERR_ARG, "bad argument"); }
+    DeviceGuard dg(plan->device);
+    std::vector<cudaEvent_t> ev(2 * n + 2);
+    for (auto& e : ev) { ck(cudaEventCreate(&e), "cudaEventCreate"); }
+    struct Rel {
+      std::vector<cudaEvent_t>& v;
+      ~Rel() { for (auto e : v) { cudaEventDestroy(e); } }
+    } rel{ev};
+    ck(cudaEventRecord(ev[0], plan->stream), "record");
+    pass1(plan, owl::P1_IN, plan->F1, buf, 0);
+    ck(cudaEventRecord(ev[1], plan->stream), "record");
+    for (uint32_t k = 0; k < n; ++k) {
+      pass2(plan, owl::P2_SQUARE, plan->F1, nullptr, nullptr);
+      ck(cudaEventRecord(ev[2 + 2 * k], plan->stream), "record");
+      if (k + 1 < n) {
+        pass1(plan, owl::P1_FUSED, plan->F1, nullptr, 0);
+      } else {
+        pass1(plan, owl::P1_OUT, plan->F1, buf, 0);
+      }
+      ck(cudaEventRecord(ev[3 + 2 * k], plan->stream), "record");
+    }
+    sync_and_check(plan);
+    float t2 = 0, t1 = 0, te = 0, x = 0;
+    ck(cudaEventElapsedTime(&x, ev[0], ev[1]), "elapsed");
+    te += x;
+    for (uint32_t k = 0; k < n; ++k) {
+      ck(cudaEventElapsedTime(&x, ev[1 + 2 * k], ev[2 + 2 * k]), "elapsed");
+      t2 += x;
+      ck(cudaEventElapsedTime(&x, ev[2 + 2 * k], ev[3 + 2 * k]), "elapsed");
+      if (k + 1 < n) { t1 += x; } else { te += x; }
+    }
+    ms[0] = t2;
+    ms[1] = t1;
+    ms[2] = te;
+    launches[0] = n;
+    launches[1] = n - 1;
+    launches[2] = 2;
+  });
+}
+
+int owl_probe_wait_timeout(owl_plan* plan) {
+  return guarded([&] {
+    check_plan(plan);
+    DeviceGuard dg(plan->device);
+    // an index past the line groups' flags that nothing ever sets: the flags
+    // array is followed by the control block, so use the Ctl padding word
+    owl::Args a = plan->args;
+    a.flags = &plan->args.ctl->pad[0];
+    ck(cudaMemsetAsync(a.flags, 0, sizeof(uint32_t), plan->stream), "clear probe flag");
+    owl::k_wait_probe<<<1, 32, 0, plan->stream>>>(a, 0);
+    ck(cudaGetLastError(), "probe launch");
+    sync_and_check(plan);
+  });
+}
+
+}  // extern "C"

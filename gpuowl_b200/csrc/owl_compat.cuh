@@ -1,0 +1,32 @@
+// owl_compat.cuh -- the few CUDA spellings the kernels use that differ when
+// the same source is compiled as host C++ for the CPU kernel emulator
+// (tests/emu, built with -DOWL_EMU). The product build never defines OWL_EMU.
+#pragma once
+
+#ifdef OWL_EMU
+#include "owl_emu_rt.hpp"
+#else
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#define OWL_DYN_SHARED(T, name) extern __shared__ T name[]
+#define OWL_SHARED(T, name) __shared__ T name
+#define OWL_SHARED_ARR(T, name, n) __shared__ T name[n]
+
+namespace owl {
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void spin_pause() { __nanosleep(20); }
+}  // namespace owl
+#endif

@@ -1,0 +1,226 @@
+// owl_dft.cuh -- FP64 complex arithmetic and small DFTs in registers, plus the
+// shared-memory Stockham stage helpers used by the two pass kernels.
+//
+// Conventions: forward DFT X[k] = sum_n x[n] w^(nk) with w = exp(-2 pi i / n);
+// INV selects w = exp(+2 pi i / n) (unnormalised). All small DFTs take and
+// return natural order.
+#pragma once
+#include <cstdint>
+#include "owl_compat.cuh"
+
+namespace owl {
+
+typedef double2 C;
+
+__device__ __forceinline__ C mk(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ C cadd(C a, C b) { return mk(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ C csub(C a, C b) { return mk(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ C cneg(C a) { return mk(-a.x, -a.y); }
+__device__ __forceinline__ C cconj(C a) { return mk(a.x, -a.y); }
+__device__ __forceinline__ C cmul(C a, C b) {
+  return mk(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// a * conj(b)
+__device__ __forceinline__ C cmulc(C a, C b) {
+  return mk(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ C csq(C a) { return mk(fma(a.x, a.x, -a.y * a.y), 2.0 * a.x * a.y); }
+// multiply by i
+__device__ __forceinline__ C cmuli(C a) { return mk(-a.y, a.x); }
+// multiply by -i
+__device__ __forceinline__ C cmulmi(C a) { return mk(a.y, -a.x); }
+
+template <bool INV> __device__ __forceinline__ C cmulw(C a, C w) { return INV ? cmulc(a, w) : cmul(a, w); }
+
+// w4 = -i (forward) / +i (inverse)
+template <bool INV> __device__ __forceinline__ C mul_w4(C a) { return INV ? cmuli(a) : cmulmi(a); }
+
+constexpr double kC1 = 0.92387953251128675613;  // cos(pi/8)
+constexpr double kS1 = 0.38268343236508977173;  // sin(pi/8)
+constexpr double kSQ = 0.70710678118654752440;  // sqrt(1/2)
+
+// a * w16^M, M a compile-time constant in [0, 16)
+template <bool INV, int M> __device__ __forceinline__ C mul_w16(C a) {
+  constexpr int m = M & 15;
+  if constexpr (m == 0) {
+    return a;
+  } else if constexpr (m == 8) {
+    return cneg(a);
+  } else if constexpr (m == 4) {
+    return mul_w4<INV>(a);
+  } else if constexpr (m == 12) {
+    return mul_w4<!INV>(a);
+  } else if constexpr (m == 2 || m == 6 || m == 10 || m == 14) {
+    // (+-1 +- i) sqrt(1/2): forward w16^2 = (1 - i)/sqrt2
+    constexpr int q = m / 2;  // 1,3,5,7 -> w8^q
+    C b = a;
+    if constexpr (q == 3) { b = mul_w4<INV>(a); }
+    if constexpr (q == 5) { b = cneg(a); }
+    if constexpr (q == 7) { b = mul_w4<!INV>(a); }
+    // b * w8^1
+    if constexpr (!INV) {
+      return mk((b.x + b.y) * kSQ, (b.y - b.x) * kSQ);
+    } else {
+      return mk((b.x - b.y) * kSQ, (b.x + b.y) * kSQ);
+    }
+  } else {
+    // odd m: full complex multiply by (cos 2pi m/16, -+sin 2pi m/16)
+    constexpr int k = m % 4;     // 1 or 3
+    constexpr int quad = m / 4;  // rotation by w4^quad
+    constexpr double c = (k == 1) ? kC1 : kS1;
+    constexpr double s = (k == 1) ? kS1 : kC1;
+    C b = a;
+    if constexpr (quad == 1) { b = mul_w4<INV>(a); }
+    if constexpr (quad == 2) { b = cneg(a); }
+    if constexpr (quad == 3) { b = mul_w4<!INV>(a); }
+    // forward: (c - i s), inverse: (c + i s)
+    if constexpr (!INV) {
+      return mk(fma(b.x, c, b.y * s), fma(b.y, c, -b.x * s));
+    } else {
+      return mk(fma(b.x, c, -b.y * s), fma(b.y, c, b.x * s));
+    }
+  }
+}
+
+template <bool INV> __device__ __forceinline__ void dft2(C* v) {
+  C a = v[0];
+  v[0] = cadd(a, v[1]);
+  v[1] = csub(a, v[1]);
+}
+
+template <bool INV> __device__ __forceinline__ void dft4s(C& x0, C& x1, C& x2, C& x3) {
+  C a = cadd(x0, x2), b = csub(x0, x2), c = cadd(x1, x3), d = mul_w4<INV>(csub(x1, x3));
+  x0 = cadd(a, c);
+  x2 = csub(a, c);
+  x1 = cadd(b, d);
+  x3 = csub(b, d);
+}
+
+template <bool INV> __device__ __forceinline__ void dft4(C* v) { dft4s<INV>(v[0], v[1], v[2], v[3]); }
+
+// 8 = 4 (over n1, stride 2) x 2
+template <bool INV> __device__ __forceinline__ void dft8(C* v) {
+  C y0 = v[0], y2 = v[2], y4 = v[4], y6 = v[6];
+  C y1 = v[1], y3 = v[3], y5 = v[5], y7 = v[7];
+  dft4s<INV>(y0, y2, y4, y6);  // Y0[k1], k1 = 0..3 in (y0, y2, y4, y6)
+  dft4s<INV>(y1, y3, y5, y7);  // Y1[k1]
+  y3 = mul_w16<INV, 2>(y3);
+  y5 = mul_w16<INV, 4>(y5);
+  y7 = mul_w16<INV, 6>(y7);
+  v[0] = cadd(y0, y1);
+  v[4] = csub(y0, y1);
+  v[1] = cadd(y2, y3);
+  v[5] = csub(y2, y3);
+  v[2] = cadd(y4, y5);
+  v[6] = csub(y4, y5);
+  v[3] = cadd(y6, y7);
+  v[7] = csub(y6, y7);
+}
+
+// 16 = 4 (over n1, stride 4) x 4
+template <bool INV> __device__ __forceinline__ void dft16(C* v) {
+  C y[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) { y[i] = v[i]; }
+  // step 1: for n2: DFT4 over n1 of x[4 n1 + n2]; result k1 kept at index n2 + 4 k1
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) { dft4s<INV>(y[n2], y[n2 + 4], y[n2 + 8], y[n2 + 12]); }
+  // step 2: twiddle w16^(n2 k1)
+  y[1 + 4 * 1] = mul_w16<INV, 1>(y[1 + 4 * 1]);
+  y[1 + 4 * 2] = mul_w16<INV, 2>(y[1 + 4 * 2]);
+  y[1 + 4 * 3] = mul_w16<INV, 3>(y[1 + 4 * 3]);
+  y[2 + 4 * 1] = mul_w16<INV, 2>(y[2 + 4 * 1]);
+  y[2 + 4 * 2] = mul_w16<INV, 4>(y[2 + 4 * 2]);
+  y[2 + 4 * 3] = mul_w16<INV, 6>(y[2 + 4 * 3]);
+  y[3 + 4 * 1] = mul_w16<INV, 3>(y[3 + 4 * 1]);
+  y[3 + 4 * 2] = mul_w16<INV, 6>(y[3 + 4 * 2]);
+  y[3 + 4 * 3] = mul_w16<INV, 9>(y[3 + 4 * 3]);
+  // step 3: for k1: DFT4 over n2 -> X[k1 + 4 k2]
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    C a = y[0 + 4 * k1], b = y[1 + 4 * k1], c = y[2 + 4 * k1], d = y[3 + 4 * k1];
+    dft4s<INV>(a, b, c, d);
+    v[k1 + 0] = a;
+    v[k1 + 4] = b;
+    v[k1 + 8] = c;
+    v[k1 + 12] = d;
+  }
+}
+
+template <int R, bool INV> __device__ __forceinline__ void dftR(C* v) {
+  if constexpr (R == 2) {
+    dft2<INV>(v);
+  } else if constexpr (R == 4) {
+    dft4<INV>(v);
+  } else if constexpr (R == 8) {
+    dft8<INV>(v);
+  } else {
+    static_assert(R == 16, "radix");
+    dft16<INV>(v);
+  }
+}
+
+// shared-memory index padding: one 16-byte pad per 2^PS elements
+template <int PS> __device__ __forceinline__ int pad(int i) { return i + (i >> PS); }
+
+constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x / 2); }
+
+// ---- Stockham stage helpers for one line of N complex values held by N/16
+// threads, 16 values per thread. Stage radix R (R divides 16): thread `tl`
+// runs butterflies j = tl + (N/16) b, b < 16/R, inputs x[j + r N/R],
+// twiddle w_(NS R)^(r (j mod NS)), outputs y[(j/NS) NS R + j mod NS + r NS].
+
+template <int R, int N, int PS> __device__ __forceinline__ void st_load(const C* buf, int tl, C* v) {
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    int j = tl + (N / 16) * b;
+#pragma unroll
+    for (int r = 0; r < R; ++r) { v[b * R + r] = buf[pad<PS>(j + r * (N / R))]; }
+  }
+}
+
+// tab: w_N^i for i < N (forward sign)
+template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twiddle(int tl, C* v, const C* __restrict__ tab) {
+  if constexpr (NS > 1) {
+#pragma unroll
+    for (int b = 0; b < 16 / R; ++b) {
+      int j = tl + (N / 16) * b;
+      int k = j & (NS - 1);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        C w = __ldg(tab + r * k * (N / (NS * R)));
+        v[b * R + r] = cmulw<INV>(v[b * R + r], w);
+      }
+    }
+  }
+}
+
+template <int R, bool INV> __device__ __forceinline__ void st_dft(C* v) {
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) { dftR<R, INV>(v + b * R); }
+}
+
+template <int R, int N, int NS, int PS> __device__ __forceinline__ void st_store(C* buf, int tl, const C* v) {
+#pragma unroll
+  for (int b = 0; b < 16 / R; ++b) {
+    int j = tl + (N / 16) * b;
+    int base = (j / NS) * NS * R + (j & (NS - 1));
+#pragma unroll
+    for (int r = 0; r < R; ++r) { buf[pad<PS>(base + r * NS)] = v[b * R + r]; }
+  }
+}
+
+// Radix plan for a line of N points whose last inverse / first forward stage
+// (radix RL) is split across lines or columns: N = R1 * M1 * M2 * RL.
+template <int N, int RL> struct Plan {
+  static constexpr int REST = N / RL;
+  static constexpr int R1 = REST >= 16 ? 16 : REST;
+  static constexpr int REST2 = REST / R1;
+  static constexpr int M1 = REST2 >= 16 ? 16 : REST2;
+  static constexpr int M2 = REST2 / M1;
+  static_assert(R1 * M1 * M2 * RL == N, "plan");
+  static_assert(M2 >= 1 && M2 <= 16, "plan depth");
+  static_assert(R1 >= 4, "first radix too small for conflict-free padding");
+};
+
+}  // namespace owl

@@ -1,0 +1,633 @@
+// owl_kernels.cuh -- the IBDWT squaring passes for sm_100a.
+//
+// One iteration x <- x^2 (-2) mod 2^E-1 over N = 2*W*H FP64 words is two HBM
+// passes over the hN = W*H complex state F (packing z[j] = x[2j] + i x[2j+1],
+// the reference's kAt(), src/Gpu.cpp:40):
+//
+//   pass 2 ("column" pass, k_pass2): for each column pair (k1, W-k1) of the
+//     W x H matrix A[k1][j2]: twiddle by w_hN^(k1 j2), forward length-H DFT,
+//     real-signal squaring of Z[k] with Z[hN-k] (reference tailSquare /
+//     pairSq, src/cl/tailsquare.cl:35-74), inverse DFT, untwiddle.
+//   pass 1 ("line" pass, k_pass1): for each group of R lines j2: inverse
+//     length-W DFT, inverse weight, round, balanced-digit carry, publish the
+//     line group's carry-out, take the predecessor's carry-in (decoupled
+//     lookback with a bounded wait), weight, forward length-W DFT (reference
+//     carryFused, src/cl/carryfused.cl:21-231).
+//
+// Layout of F in HBM: tiles of R lines x one column pair. Element (column k1,
+// line j2) lives at (((j2/R) * (W/2) + c) * 2 + s) * R + j2 % R where the pair
+// index c and side s are c = k1, s = 0 for 0 < k1 < W/2; c = W-k1, s = 1 for
+// k1 > W/2; (0,0) for k1 = 0 and (0,1) for k1 = W/2. Pass 1 reads one
+// contiguous block of R*W elements; pass 2 reads 2*R contiguous elements per
+// line group, and each 32-byte sector it touches is used whole.
+#pragma once
+#include "owl_compat.cuh"
+#include "owl_dft.cuh"
+
+namespace owl {
+
+struct Ctl {
+  uint32_t ticket;  // line-group ticket for the carry chain (reset by the last taker)
+  uint32_t error;   // OWL_DEVERR_* bits, sticky until the host clears them
+  uint32_t pad[30];
+};
+
+enum : uint32_t { DEVERR_WAIT = 1u };
+
+struct Args {
+  const C* twW;    // w_W^i, i < W
+  const C* twH;    // w_H^i, i < H
+  const C* twLo;   // w_hN^i, i < 2^loShift
+  const C* twHi;   // w_hN^(i << loShift)
+  const double* wt1;   // per column j1: 2^(X1/N)
+  const double* iwt1;  // per column j1: 2^(-X1/N)
+  const uint32_t* x1;  // per column j1: X1 = step*2H*j1 mod N
+  const double* wt2;   // per (line j2, e): 2^(X2/N)
+  const double* iwt2;  // per (line j2, e): 2^(-X2/N) / (4 hN)
+  const uint32_t* x2;  // per (line j2, e): X2 = step*(2 j2 + e) mod N
+  long long* shuttle;  // carry rows, (H/R) x W
+  uint32_t* flags;     // per line group
+  Ctl* ctl;
+  float* roe;          // per-launch max round-off slots
+  uint32_t E, N, W, H, hN;
+  uint32_t bitsLo;     // E / N
+  uint32_t eModN;      // E % N (a word is big iff its extra < E % N)
+  uint32_t loShift;
+  unsigned long long timeoutNs;
+};
+
+enum : int { P1_FUSED = 0, P1_IN = 1, P1_OUT = 2 };
+
+// smem strides: room for the largest padding used (one pad per 2^PS elements,
+// PS >= 2), rounded so that consecutive lines start 4 elements apart mod 8
+template <int W, int R> constexpr int p1_line_stride() {
+  constexpr int ps = ilog2(16 / R) < ilog2(Plan<W, 16 / R>::R1) ? ilog2(16 / R) : ilog2(Plan<W, 16 / R>::R1);
+  return W + (W >> ps) + 4;
+}
+template <int H> constexpr int p2_col_stride() { return H + (H >> 3) + 4; }
+enum : int { P2_SQUARE = 0, P2_FWD = 1, P2_MUL = 2 };
+enum : int { FL_MUL3 = 1, FL_LL = 2 };
+
+template <int R> __device__ __forceinline__ uint32_t faddr(uint32_t W, uint32_t j2, uint32_t c, uint32_t s) {
+  return (((j2 / R) * (W / 2) + c) * 2 + s) * R + (j2 % R);
+}
+// pair index and side of column k1
+__device__ __forceinline__ void colpair(uint32_t W, uint32_t k1, uint32_t& c, uint32_t& s) {
+  if (k1 == 0) {
+    c = 0; s = 0;
+  } else if (k1 == W / 2) {
+    c = 0; s = 1;
+  } else if (k1 < W / 2) {
+    c = k1; s = 0;
+  } else {
+    c = W - k1; s = 1;
+  }
+}
+
+// w_hN^m, m < hN, from the two-level table (one rounding in the product)
+__device__ __forceinline__ C bigtw(const Args& a, uint32_t m) {
+  C lo = __ldg(a.twLo + (m & ((1u << a.loShift) - 1)));
+  C hi = __ldg(a.twHi + (m >> a.loShift));
+  return cmul(lo, hi);
+}
+
+__device__ __forceinline__ long long sext_low(long long x, uint32_t bits) {
+  return (long long)((unsigned long long)x << (64 - bits)) >> (64 - bits);
+}
+
+constexpr double RNDVAL = 3.0 * 2251799813685248.0;  // 3 * 2^51
+
+// ---------------------------------------------------------------------------
+// Pass 1: R lines of W points per CTA, R*W/16 threads, 16 values per thread.
+template <int W, int R, int MODE>
+__global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
+    k_pass1(Args a, C* __restrict__ F, int32_t* __restrict__ words, int roeSlot, int flags) {
+  constexpr int T = R * W / 16;
+  constexpr int RL = 16 / R;
+  using P = Plan<W, RL>;
+  constexpr int PS_R1 = ilog2(P::R1);
+  constexpr int PS_RL = ilog2(RL);
+  constexpr int LS = p1_line_stride<W, R>();  // line stride in smem (elements), == 4 mod 8
+  OWL_DYN_SHARED(C, smem);
+  OWL_SHARED(uint32_t, s_g);
+  OWL_SHARED_ARR(float, s_roe, 32);
+
+  const int t = threadIdx.x;
+  const uint32_t G = a.H / R;
+  uint32_t g;
+  if (MODE == P1_IN) {
+    g = blockIdx.x;
+  } else {
+    if (t == 0) {
+      uint32_t tk = atomicAdd(&a.ctl->ticket, 1u);
+      if (tk == G - 1) { atomicExch(&a.ctl->ticket, 0u); }
+      s_g = tk;
+    }
+    __syncthreads();
+    g = s_g;
+  }
+
+  // per-line mapping for the inner stages
+  const int l = t % R;
+  const int tl = t / R;
+  C* line = smem + l * LS;
+
+  C v[16];  // cross-line layout: v[ll * RL + r] = line ll, column j1 = t + (W/RL) r
+  float roe = 0.0f;
+
+  if constexpr (MODE != P1_IN) {
+    // ---- inverse width DFT ----
+    {
+      C u[16];
+#pragma unroll
+      for (int b = 0; b < 16 / P::R1; ++b) {
+        int j = tl + (W / 16) * b;
+#pragma unroll
+        for (int r = 0; r < P::R1; ++r) {
+          uint32_t k1 = j + r * (W / P::R1), c, s;
+          colpair(W, k1, c, s);
+          u[b * P::R1 + r] = F[faddr<R>(W, g * R + l, c, s)];
+        }
+      }
+      st_dft<P::R1, true>(u);
+      st_store<P::R1, W, 1, PS_R1>(line, tl, u);
+      __syncthreads();
+      constexpr int NS2 = P::R1;
+      constexpr int PS_AFTER_M1 = (P::M1 > 1) ? 4 : PS_R1;
+      if constexpr (P::M1 > 1) {
+        st_load<P::M1, W, PS_R1>(line, tl, u);
+        st_twiddle<P::M1, W, NS2, true>(tl, u, a.twW);
+        st_dft<P::M1, true>(u);
+        __syncthreads();
+        st_store<P::M1, W, NS2, 4>(line, tl, u);
+        __syncthreads();
+      }
+      constexpr int NS3 = NS2 * P::M1;
+      constexpr int PS_AFTER_M2 = (P::M2 > 1) ? 4 : PS_AFTER_M1;
+      if constexpr (P::M2 > 1) {
+        st_load<P::M2, W, PS_AFTER_M1>(line, tl, u);
+        st_twiddle<P::M2, W, NS3, true>(tl, u, a.twW);
+        st_dft<P::M2, true>(u);
+        __syncthreads();
+        st_store<P::M2, W, NS3, 4>(line, tl, u);
+        __syncthreads();
+      }
+      // last stage, radix RL, across the R lines: butterfly j = t of every line
+      constexpr int NSL = W / RL;
+#pragma unroll
+      for (int ll = 0; ll < R; ++ll) {
+        const C* ln = smem + ll * LS;
+#pragma unroll
+        for (int r = 0; r < RL; ++r) { v[ll * RL + r] = ln[pad<PS_AFTER_M2>(t + r * NSL)]; }
+        if constexpr (NSL > 1) {
+#pragma unroll
+          for (int r = 1; r < RL; ++r) { v[ll * RL + r] = cmulw<true>(v[ll * RL + r], __ldg(a.twW + r * t)); }
+        }
+        dftR<RL, true>(v + ll * RL);
+      }
+    }
+  }
+
+  // ---- words: inverse weight, round, carry (or load digits for P1_IN) ----
+  long long dig[R][RL][2];
+  uint32_t bigmask = 0;  // bit (r*R + ll)*2 + e
+#pragma unroll
+  for (int r = 0; r < RL; ++r) {
+    const uint32_t j1 = t + (W / RL) * r;
+    const uint32_t X1 = __ldg(a.x1 + j1);
+    if constexpr (MODE == P1_IN) {
+      // digits in natural word order: word 2(H j1 + j2) + e
+#pragma unroll
+      for (int ll = 0; ll < R; ++ll) {
+        uint32_t j2 = g * R + ll;
+        int2 w2 = *reinterpret_cast<const int2*>(words + 2 * ((size_t)a.H * j1 + j2));
+        dig[ll][r][0] = w2.x;
+        dig[ll][r][1] = w2.y;
+      }
+    } else {
+      const double iw1 = __ldg(a.iwt1 + j1);
+      long long carry = ((flags & FL_LL) && g == 0 && j1 == 0) ? -2 : 0;
+#pragma unroll
+      for (int ll = 0; ll < R; ++ll) {
+        uint32_t j2 = g * R + ll;
+        C z = v[ll * RL + r];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          uint32_t X2 = __ldg(a.x2 + 2 * j2 + e);
+          uint32_t sum = X1 + X2;
+          bool wrap = sum >= a.N;
+          uint32_t extra = wrap ? sum - a.N : sum;
+          bool big = extra < a.eModN;
+          if (big) { bigmask |= 1u << ((r * R + ll) * 2 + e); }
+          uint32_t bits = a.bitsLo + (big ? 1 : 0);
+          double iw = iw1 * __ldg(a.iwt2 + 2 * j2 + e);
+          if (wrap) { iw *= 2.0; }
+          double x = e ? z.y : z.x;
+          double d = fma(x, iw, RNDVAL);
+          double rv = d - RNDVAL;
+          roe = fmaxf(roe, (float)fabs(fma(x, iw, -rv)));
+          long long n = __double_as_longlong(d) - __double_as_longlong(RNDVAL);
+          if (flags & FL_MUL3) { n *= 3; }
+          long long xx = n + carry;
+          long long dd = sext_low(xx, bits);
+          carry = (xx - dd) >> bits;
+          dig[ll][r][e] = dd;
+        }
+      }
+      a.shuttle[(size_t)g * W + j1] = carry;
+    }
+  }
+
+  if constexpr (MODE != P1_IN) {
+    // publish this group's carry row, then take the predecessor's
+    __threadfence();
+    // ROE: block max
+    constexpr unsigned WMASK = (T >= 32) ? 0xffffffffu : ((1u << T) - 1u);
+#pragma unroll
+    for (int o = (T >= 32 ? 16 : T / 2); o > 0; o >>= 1) { roe = fmaxf(roe, __shfl_xor_sync(WMASK, roe, o)); }
+    if ((t & 31) == 0) { s_roe[t >> 5] = roe; }
+    __syncthreads();
+    if (t == 0) {
+      st_release(a.flags + g, 1u);
+      float m = 0.0f;
+      for (int i = 0; i < (T + 31) / 32; ++i) { m = fmaxf(m, s_roe[i]); }
+      if (a.roe != nullptr && roeSlot >= 0) { atomicMax(reinterpret_cast<unsigned int*>(a.roe) + roeSlot, __float_as_uint(m)); }
+      const uint32_t prev = (g == 0) ? G - 1 : g - 1;
+      unsigned long long t0 = gtimer();
+      bool ok = false;
+      for (uint32_t it = 0; it < (1u << 30); ++it) {
+        if (ld_acquire(a.flags + prev) != 0u) { ok = true; break; }
+        if ((it & 255u) == 255u && gtimer() - t0 > a.timeoutNs) { break; }
+        spin_pause();
+      }
+      if (ok) {
+        a.flags[prev] = 0u;
+      } else {
+        atomicOr(&a.ctl->error, DEVERR_WAIT);
+      }
+    }
+    __syncthreads();
+    // carry-in for line 0 of this group (carryFinal, src/cl/carryinc.cl:18-23)
+    const uint32_t prevg = (g == 0) ? G - 1 : g - 1;
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const uint32_t j1 = t + (W / RL) * r;
+      uint32_t src = (g == 0) ? (j1 == 0 ? W - 1 : j1 - 1) : j1;
+      long long cin = __ldcg(a.shuttle + (size_t)prevg * W + src);
+      uint32_t bits0 = a.bitsLo + ((bigmask >> ((r * R + 0) * 2 + 0)) & 1u);
+      long long xx = dig[0][r][0] + cin;
+      long long dd = sext_low(xx, bits0);
+      dig[0][r][0] = dd;
+      dig[0][r][1] += (xx - dd) >> bits0;
+    }
+  }
+
+  if constexpr (MODE == P1_OUT) {
+    // digits to natural word order
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const uint32_t j1 = t + (W / RL) * r;
+#pragma unroll
+      for (int ll = 0; ll < R; ++ll) {
+        uint32_t j2 = g * R + ll;
+        int2 w2 = make_int2((int)dig[ll][r][0], (int)dig[ll][r][1]);
+        *reinterpret_cast<int2*>(words + 2 * ((size_t)a.H * j1 + j2)) = w2;
+      }
+    }
+    return;
+  } else {
+    // ---- weight ----
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const uint32_t j1 = t + (W / RL) * r;
+      const uint32_t X1 = __ldg(a.x1 + j1);
+      const double w1 = __ldg(a.wt1 + j1);
+#pragma unroll
+      for (int ll = 0; ll < R; ++ll) {
+        uint32_t j2 = g * R + ll;
+        double y[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          uint32_t X2 = __ldg(a.x2 + 2 * j2 + e);
+          double w = w1 * __ldg(a.wt2 + 2 * j2 + e);
+          if (X1 + X2 >= a.N) { w *= 0.5; }
+          y[e] = (double)dig[ll][r][e] * w;
+        }
+        v[ll * RL + r] = mk(y[0], y[1]);
+      }
+    }
+    // ---- forward width DFT: first stage across lines from registers ----
+    if constexpr (MODE != P1_IN) { __syncthreads(); }  // smem still being read by the last inverse stage
+#pragma unroll
+    for (int ll = 0; ll < R; ++ll) {
+      dftR<RL, false>(v + ll * RL);
+      C* ln = smem + ll * LS;
+#pragma unroll
+      for (int r = 0; r < RL; ++r) { ln[pad<PS_RL>(t * RL + r)] = v[ll * RL + r]; }
+    }
+    __syncthreads();
+    C u[16];
+    constexpr int NSa = RL;
+    constexpr int PS_A = (P::M2 > 1) ? 4 : PS_RL;
+    if constexpr (P::M2 > 1) {
+      st_load<P::M2, W, PS_RL>(line, tl, u);
+      st_twiddle<P::M2, W, NSa, false>(tl, u, a.twW);
+      st_dft<P::M2, false>(u);
+      __syncthreads();
+      st_store<P::M2, W, NSa, 4>(line, tl, u);
+      __syncthreads();
+    }
+    constexpr int NSb = NSa * P::M2;
+    constexpr int PS_B = (P::M1 > 1) ? 4 : PS_A;
+    if constexpr (P::M1 > 1) {
+      st_load<P::M1, W, PS_A>(line, tl, u);
+      st_twiddle<P::M1, W, NSb, false>(tl, u, a.twW);
+      st_dft<P::M1, false>(u);
+      __syncthreads();
+      st_store<P::M1, W, NSb, 4>(line, tl, u);
+      __syncthreads();
+    }
+    constexpr int NSc = NSb * P::M1;  // == W / R1
+    st_load<P::R1, W, PS_B>(line, tl, u);
+    st_twiddle<P::R1, W, NSc, false>(tl, u, a.twW);
+    st_dft<P::R1, false>(u);
+    // outputs k1 = j + r (W/R1) straight to HBM
+#pragma unroll
+    for (int b = 0; b < 16 / P::R1; ++b) {
+      int j = tl + (W / 16) * b;
+#pragma unroll
+      for (int r = 0; r < P::R1; ++r) {
+        uint32_t k1 = j + r * (W / P::R1), c, s;
+        colpair(W, k1, c, s);
+        F[faddr<R>(W, g * R + l, c, s)] = u[b * P::R1 + r];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass 2: one column pair (A: k1 = c, B: k1 = W - c; pair 0 is (0, W/2)) of H
+// points per CTA, H/8 threads. Per-column stages use threads [0, H/16) for A
+// and [H/16, H/8) for B; the last forward / first inverse stage (radix 8) runs
+// butterfly j = t of A and j = H/8-1-t of B in the same thread, so that the
+// thread ends up holding A[k2] and its partner B[H-1-k2] (src/cl/tailsquare.cl
+// pairs lines k and H-k the same way, 225-313).
+
+// real-signal squaring of the pair (a = Z[k], b = Z[hN-k]) with t2 = w_hN^k:
+// returns 4 W[k] in a and 4 W[hN-k] in b.
+__device__ __forceinline__ void pair_sq(C& a, C& b, C t2) {
+  C bc = cconj(b);
+  C e2 = cadd(a, bc);
+  C o2 = cmulmi(csub(a, bc));
+  C s = cadd(csq(e2), cmul(t2, csq(o2)));
+  C p = cmuli(cmul(e2, o2));
+  p = mk(2.0 * p.x, 2.0 * p.y);
+  a = cadd(s, p);
+  b = cconj(csub(s, p));
+}
+
+// product of two signals: (a, b) pair of the first, (c, d) of the second
+__device__ __forceinline__ void pair_mul(C& a, C& b, C c, C d, C t2) {
+  C bc = cconj(b), dc = cconj(d);
+  C e2a = cadd(a, bc), o2a = cmulmi(csub(a, bc));
+  C e2b = cadd(c, dc), o2b = cmulmi(csub(c, dc));
+  C s = cadd(cmul(e2a, e2b), cmul(t2, cmul(o2a, o2b)));
+  C p = cmuli(cadd(cmul(e2a, o2b), cmul(o2a, e2b)));
+  a = cadd(s, p);
+  b = cconj(csub(s, p));
+}
+
+// one-sided version for the self-paired columns 0 and W/2 (a = Z[k], b = Z[partner])
+__device__ __forceinline__ C one_sq(C a, C b, C t2) {
+  C bc = cconj(b);
+  C e2 = cadd(a, bc);
+  C o2 = cmulmi(csub(a, bc));
+  C s = cadd(csq(e2), cmul(t2, csq(o2)));
+  C p = cmuli(cmul(e2, o2));
+  return cadd(s, mk(2.0 * p.x, 2.0 * p.y));
+}
+__device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
+  C bc = cconj(b), dc = cconj(d);
+  C e2a = cadd(a, bc), o2a = cmulmi(csub(a, bc));
+  C e2b = cadd(c, dc), o2b = cmulmi(csub(c, dc));
+  C s = cadd(cmul(e2a, e2b), cmul(t2, cmul(o2a, o2b)));
+  C p = cmuli(cadd(cmul(e2a, o2b), cmul(o2a, e2b)));
+  return cadd(s, p);
+}
+
+template <int H, int R, int MODE>
+__global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
+    k_pass2(Args a, C* __restrict__ F, const C* __restrict__ Fb, C* __restrict__ Fq) {
+  constexpr int T = H / 8;
+  constexpr int TC = H / 16;  // threads per column in the per-column stages
+  using P = Plan<H, 8>;
+  constexpr int PS_R1 = ilog2(P::R1);
+  constexpr int CS = p2_col_stride<H>();
+  OWL_DYN_SHARED(C, smem);
+
+  const uint32_t W = a.W;
+  const uint32_t c = blockIdx.x;
+  const int t = threadIdx.x;
+  const int col = t / TC;
+  const int tc = t % TC;
+  const uint32_t kA = c, kB = (c == 0) ? W / 2 : W - c;
+  (void)a.E;
+  const uint32_t k1 = col ? kB : kA;
+  C* cbuf = smem + col * CS;
+
+  C u[16];
+  // ---- forward column DFT, first stage from HBM with the w_hN^(k1 j2) twiddle ----
+#pragma unroll
+  for (int b = 0; b < 16 / P::R1; ++b) {
+    int j = tc + TC * b;
+#pragma unroll
+    for (int r = 0; r < P::R1; ++r) {
+      uint32_t j2 = j + r * (H / P::R1);
+      C x = F[faddr<R>(W, j2, c, col)];
+      u[b * P::R1 + r] = cmul(x, bigtw(a, k1 * j2));
+    }
+  }
+  st_dft<P::R1, false>(u);
+  st_store<P::R1, H, 1, PS_R1>(cbuf, tc, u);
+  __syncthreads();
+  constexpr int PS_AFTER_M1 = (P::M1 > 1) ? 4 : PS_R1;
+  if constexpr (P::M1 > 1) {
+    st_load<P::M1, H, PS_R1>(cbuf, tc, u);
+    st_twiddle<P::M1, H, P::R1, false>(tc, u, a.twH);
+    st_dft<P::M1, false>(u);
+    __syncthreads();
+    st_store<P::M1, H, P::R1, 4>(cbuf, tc, u);
+    __syncthreads();
+  }
+  constexpr int PS_AFTER_M2 = (P::M2 > 1) ? 4 : PS_AFTER_M1;
+  if constexpr (P::M2 > 1) {
+    st_load<P::M2, H, PS_AFTER_M1>(cbuf, tc, u);
+    st_twiddle<P::M2, H, P::R1 * P::M1, false>(tc, u, a.twH);
+    st_dft<P::M2, false>(u);
+    __syncthreads();
+    st_store<P::M2, H, P::R1 * P::M1, 4>(cbuf, tc, u);
+    __syncthreads();
+  }
+  // last forward stage (radix 8, NS = H/8 = T): A butterfly t, B butterfly T-1-t
+  const int jB = T - 1 - t;
+  C* bufA = smem;
+  C* bufB = smem + CS;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    u[r] = bufA[pad<PS_AFTER_M2>(t + r * T)];
+    u[8 + r] = bufB[pad<PS_AFTER_M2>(jB + r * T)];
+  }
+  if constexpr (T > 1) {
+#pragma unroll
+    for (int r = 1; r < 8; ++r) {
+      u[r] = cmul(u[r], __ldg(a.twH + r * t));
+      u[8 + r] = cmul(u[8 + r], __ldg(a.twH + r * jB));
+    }
+  }
+  dft8<false>(u);
+  dft8<false>(u + 8);
+  // now u[r] = ZA[t + T r], u[8 + r] = ZB[jB + T r]
+
+  if constexpr (MODE == P2_FWD) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      uint32_t kA2 = t + T * r, kB2 = jB + T * r;
+      Fq[faddr<R>(W, kA2, c, 0)] = u[r];
+      Fq[faddr<R>(W, kB2, c, 1)] = u[8 + r];
+    }
+    return;
+  } else {
+    if (c != 0) {
+      const C tA = bigtw(a, kA);  // w_hN^c
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        uint32_t k2 = t + T * r;  // A index; partner is B[H-1-k2] = u[8 + 7 - r]
+        C t2 = cmul(tA, __ldg(a.twH + k2));
+        if constexpr (MODE == P2_SQUARE) {
+          pair_sq(u[r], u[15 - r], t2);
+        } else {
+          C cA = Fb[faddr<R>(W, k2, c, 0)];
+          C cB = Fb[faddr<R>(W, H - 1 - k2, c, 1)];
+          pair_mul(u[r], u[15 - r], cA, cB, t2);
+        }
+      }
+    } else {
+      // columns 0 and W/2 pair with themselves: exchange through smem
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        bufA[t + T * r] = u[r];
+        bufB[jB + T * r] = u[8 + r];
+      }
+      __syncthreads();
+      const C tB = bigtw(a, W / 2);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        uint32_t kA2 = t + T * r;
+        uint32_t pA = (H - kA2) & (H - 1);
+        uint32_t kB2 = jB + T * r;
+        uint32_t pB = H - 1 - kB2;
+        C t2A = __ldg(a.twH + kA2);
+        C t2B = cmul(tB, __ldg(a.twH + kB2));
+        if constexpr (MODE == P2_SQUARE) {
+          u[r] = one_sq(u[r], bufA[pA], t2A);
+          u[8 + r] = one_sq(u[8 + r], bufB[pB], t2B);
+        } else {
+          C cA = Fb[faddr<R>(W, kA2, 0, 0)], dA = Fb[faddr<R>(W, pA, 0, 0)];
+          C cB = Fb[faddr<R>(W, kB2, 0, 1)], dB = Fb[faddr<R>(W, pB, 0, 1)];
+          u[r] = one_mul(u[r], bufA[pA], cA, dA, t2A);
+          u[8 + r] = one_mul(u[8 + r], bufB[pB], cB, dB, t2B);
+        }
+      }
+    }
+    // ---- inverse column DFT: first stage (radix 8, NS = 1) from registers ----
+    dft8<true>(u);
+    dft8<true>(u + 8);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      bufA[pad<3>(t * 8 + r)] = u[r];
+      bufB[pad<3>(jB * 8 + r)] = u[8 + r];
+    }
+    __syncthreads();
+    constexpr int PS_I1 = (P::M2 > 1) ? 4 : 3;
+    if constexpr (P::M2 > 1) {
+      st_load<P::M2, H, 3>(cbuf, tc, u);
+      st_twiddle<P::M2, H, 8, true>(tc, u, a.twH);
+      st_dft<P::M2, true>(u);
+      __syncthreads();
+      st_store<P::M2, H, 8, 4>(cbuf, tc, u);
+      __syncthreads();
+    }
+    constexpr int NSi = 8 * P::M2;
+    constexpr int PS_I2 = (P::M1 > 1) ? 4 : PS_I1;
+    if constexpr (P::M1 > 1) {
+      st_load<P::M1, H, PS_I1>(cbuf, tc, u);
+      st_twiddle<P::M1, H, NSi, true>(tc, u, a.twH);
+      st_dft<P::M1, true>(u);
+      __syncthreads();
+      st_store<P::M1, H, NSi, 4>(cbuf, tc, u);
+      __syncthreads();
+    }
+    constexpr int NSl = NSi * P::M1;  // == H / R1
+    st_load<P::R1, H, PS_I2>(cbuf, tc, u);
+    st_twiddle<P::R1, H, NSl, true>(tc, u, a.twH);
+    st_dft<P::R1, true>(u);
+#pragma unroll
+    for (int b = 0; b < 16 / P::R1; ++b) {
+      int j = tc + TC * b;
+#pragma unroll
+      for (int r = 0; r < P::R1; ++r) {
+        uint32_t j2 = j + r * (H / P::R1);
+        F[faddr<R>(W, j2, c, col)] = cmulc(u[b * P::R1 + r], bigtw(a, k1 * j2));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// small helpers
+
+// out[0] &= (a == b) over n int32 (outEq must hold 1 on entry)
+__global__ void k_is_equal(const int32_t* __restrict__ a, const int32_t* __restrict__ b, size_t n, int* outEq) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t stride = (size_t)gridDim.x * blockDim.x;
+  bool eq = true;
+  for (; i < n; i += stride) { eq &= (a[i] == b[i]); }
+  if (!__all_sync(0xffffffffu, eq)) {
+    if ((threadIdx.x & 31) == 0) { atomicAnd(outEq, 0); }
+  }
+}
+
+// 64-bit checksum of n int32 taken as n/2 u64 (reference sum64, src/cl/etc.cl:19-29)
+__global__ void k_sum64(const unsigned long long* __restrict__ in, size_t n64, unsigned long long* out) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t stride = (size_t)gridDim.x * blockDim.x;
+  unsigned long long s = 0;
+  for (; i < n64; i += stride) { s += in[i]; }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) { s += __shfl_xor_sync(0xffffffffu, s, o); }
+  if ((threadIdx.x & 31) == 0) { atomicAdd(out, s); }
+}
+
+// words around the wrap: out[i] = data[(N - 32 + i) mod N], i < 64
+__global__ void k_gather_residue(const int32_t* __restrict__ data, uint32_t N, int32_t* out) {
+  int i = threadIdx.x;
+  if (i < 64) { out[i] = data[(N - 32 + i) % N]; }
+}
+
+// timeout probe: wait on a flag that is never set, with the pass-1 wait loop
+__global__ void k_wait_probe(Args a, uint32_t flagIndex) {
+  if (threadIdx.x == 0) {
+    unsigned long long t0 = gtimer();
+    bool ok = false;
+    for (uint32_t it = 0; it < (1u << 30); ++it) {
+      if (ld_acquire(a.flags + flagIndex) != 0u) { ok = true; break; }
+      if ((it & 255u) == 255u && gtimer() - t0 > a.timeoutNs) { break; }
+      spin_pause();
+    }
+    if (!ok) { atomicOr(&a.ctl->error, DEVERR_WAIT); }
+  }
+}
+
+}  // namespace owl

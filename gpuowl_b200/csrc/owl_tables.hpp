@@ -1,0 +1,127 @@
+// owl_tables.hpp -- host-side tables for one (E, W, H) shape: twiddles, the
+// IBDWT weights factored per column and per line, and the big-word data.
+//
+// Word model (reference src/state.h:14-17): N = 2 W H words, step = N - E mod N,
+// extra(k) = step k mod N, word k is big (one more bit) iff extra(k) < E mod N,
+// weight(k) = 2^(extra(k)/N) (src/Gpu.cpp:42-56). Complex element j = j2 + H j1
+// (line j2, column j1) holds words 2j and 2j+1 (src/Gpu.cpp:40 kAt), so
+// extra(2j+e) = (X1[j1] + X2[2 j2 + e]) mod N with X1 = step 2H j1 mod N and
+// X2 = step (2 j2 + e) mod N; the weight is the product of the two table
+// factors, halved when X1 + X2 >= N.
+//
+// Twiddles are evaluated in long double after an exact octant reduction of the
+// angle and rounded once to double (the reference builds its tables in long
+// double too, src/TrigBufCache.cpp:22-120).
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <stdexcept>
+#include <utility>
+#include <vector>
+
+namespace owl {
+
+struct HostC {
+  double x, y;
+};
+
+// cos and sin of 2 pi k / n
+inline void root_ld(uint64_t n, uint64_t k, long double* c, long double* s) {
+  const long double PI_L = 3.141592653589793238462643383279502884L;
+  uint64_t q = 8 * n, p = 8 * (k % n);
+  bool negS = false, negC = false, swp = false;
+  if (2 * p > q) { p = q - p; negS = true; }
+  if (4 * p > q) { p = q / 2 - p; negC = true; }
+  if (8 * p > q) { p = q / 4 - p; swp = true; }
+  long double a = 2.0L * PI_L * (long double)p / (long double)q;
+  long double cc = cosl(a), ss = sinl(a);
+  if (swp) { std::swap(cc, ss); }
+  if (negC) { cc = -cc; }
+  if (negS) { ss = -ss; }
+  *c = cc;
+  *s = ss;
+}
+
+// forward root w_n^k = exp(-2 pi i k / n)
+inline HostC root(uint64_t n, uint64_t k) {
+  long double c, s;
+  root_ld(n, k, &c, &s);
+  return HostC{(double)c, (double)-s};
+}
+
+inline bool is_pow2(uint32_t x) { return x && !(x & (x - 1)); }
+inline uint32_t log2u(uint32_t x) {
+  uint32_t r = 0;
+  while ((1u << r) < x) { ++r; }
+  return r;
+}
+
+struct Tables {
+  uint32_t E = 0, N = 0, W = 0, H = 0, hN = 0, loShift = 0;
+  std::vector<HostC> twW, twH, twLo, twHi;
+  std::vector<double> wt1, iwt1, wt2, iwt2;
+  std::vector<uint32_t> x1, x2;
+};
+
+inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
+  if (!is_pow2(W) || !is_pow2(H)) { throw std::invalid_argument("W and H must be powers of two"); }
+  Tables t;
+  t.E = E;
+  t.W = W;
+  t.H = H;
+  t.hN = W * H;
+  t.N = 2 * W * H;
+  const uint32_t N = t.N;
+  t.loShift = (log2u(t.hN) + 1) / 2;
+  t.twW.resize(W);
+  for (uint32_t i = 0; i < W; ++i) { t.twW[i] = root(W, i); }
+  t.twH.resize(H);
+  for (uint32_t i = 0; i < H; ++i) { t.twH[i] = root(H, i); }
+  uint32_t S = 1u << t.loShift;
+  t.twLo.resize(S);
+  for (uint32_t i = 0; i < S; ++i) { t.twLo[i] = root(t.hN, i); }
+  uint32_t nHi = (t.hN + S - 1) / S;
+  t.twHi.resize(nHi);
+  for (uint32_t i = 0; i < nHi; ++i) { t.twHi[i] = root(t.hN, (uint64_t)i * S); }
+
+  const uint64_t step = N - (E % N);
+  t.x1.resize(W);
+  t.wt1.resize(W);
+  t.iwt1.resize(W);
+  for (uint32_t j1 = 0; j1 < W; ++j1) {
+    uint32_t X = (uint32_t)((step * 2 * H * (uint64_t)j1) % N);
+    t.x1[j1] = X;
+    t.wt1[j1] = (double)exp2l((long double)X / N);
+    t.iwt1[j1] = (double)exp2l(-(long double)X / N);
+  }
+  t.x2.resize(2 * H);
+  t.wt2.resize(2 * H);
+  t.iwt2.resize(2 * H);
+  const long double norm = 1.0L / (4.0L * (long double)t.hN);
+  for (uint32_t i = 0; i < 2 * H; ++i) {
+    uint32_t X = (uint32_t)((step * (uint64_t)i) % N);
+    t.x2[i] = X;
+    t.wt2[i] = (double)exp2l((long double)X / N);
+    t.iwt2[i] = (double)(exp2l(-(long double)X / N) * norm);
+  }
+  return t;
+}
+
+// Shapes this build supports: W, H powers of two in [64, 4096], H >= W.
+// Smallest N = 2 W H whose bits per word E/N stays at or below `maxBpw`.
+inline bool choose_shape(uint32_t E, double maxBpw, uint32_t* W, uint32_t* H) {
+  for (uint32_t lg = 13; lg <= 25; ++lg) {
+    uint32_t N = 1u << lg;
+    if ((double)E / N > maxBpw) { continue; }
+    uint32_t hN = N / 2;
+    uint32_t w = 1u << ((lg - 1) / 2);
+    uint32_t h = hN / w;
+    if (w < 64 || h > 4096) { return false; }
+    *W = w;
+    *H = h;
+    return true;
+  }
+  return false;
+}
+
+}  // namespace owl

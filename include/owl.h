@@ -1,0 +1,128 @@
+/*
+ * owl.h -- C ABI of libowl, the B200 (sm_100a) engine for the PRP/LL iteration
+ * x <- x^2 (or x^2 - 2) mod 2^E - 1 as an IBDWT squaring with fused carry.
+ *
+ * This boundary replaces the reference's OpenCL device layer (clwrap/Kernel/
+ * KernelCompiler/Queue/Buffer, reference src/clwrap.h:54-68, src/Kernel.h:17-79,
+ * src/Queue.h:41-53, src/Buffer.h:16-102) and the kernel-level methods of its
+ * Gpu class (src/Gpu.h:213-300). Plain C types only; every call returns an int
+ * status (OWL_OK or a negative OWL_ERR_*), where the reference threw strings
+ * (src/clwrap.cpp:57-62) -- owl_error_string() and owl_last_error() give text.
+ *
+ * Data model. A "word buffer" is N int32 balanced digits in natural word order
+ * on the plan's device (the reference's Buffer<int> bufData/bufCheck/bufAux,
+ * src/Gpu.h:165-175; the reference keeps them in a transposed device layout and
+ * converts in transposeIn/Out, src/cl/transpose.cl:31-40 -- here the natural
+ * order is the device layout). Compact words are the E-bit little-endian u32
+ * form of src/state.cpp:26-69 (nWords = (E-1)/32+1).
+ *
+ * Threading: a plan owns one CUDA stream and its FFT work buffers; calls on the
+ * same plan must not run concurrently. Different plans (same or different
+ * devices) are independent.
+ */
+#ifndef OWL_H
+#define OWL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OWL_ABI_VERSION 1
+
+enum {
+  OWL_OK = 0,
+  OWL_ERR_ARG = -1,      /* bad argument / shape not supported */
+  OWL_ERR_NOMEM = -2,    /* device or host allocation failed (reference: bad_alloc, src/clwrap.cpp:286-293) */
+  OWL_ERR_CUDA = -3,     /* CUDA runtime error */
+  OWL_ERR_TIMEOUT = -4,  /* a device-side wait (carry lookback) gave up; results of that call are invalid */
+  OWL_ERR_NODEV = -5,    /* no such device */
+  OWL_ERR_READ = -6      /* checked read failed 3 times (reference "GPU persistent read errors", src/Gpu.cpp:677-705) */
+};
+
+/* flags for owl_square */
+#define OWL_SQ_MUL3 1u /* multiply the result of the LAST squaring by 3 (src/Gpu.cpp:936-945 doTailMul3) */
+#define OWL_SQ_LL 2u   /* LL step x^2 - 2 on every squaring (src/Gpu.cpp:1586-1663, src/cl/carryfused.cl:120-123) */
+
+typedef struct owl_plan owl_plan;
+
+int owl_abi_version(void);
+const char* owl_error_string(int status);
+/* text of the last error raised on this thread */
+const char* owl_last_error(void);
+
+/* Device enumeration -- reference getAllDeviceIDs/getDevice/Context (src/clwrap.h:54-68,
+   src/clwrap.cpp:189-200). pci_bus_id replaces the AMD sysfs lookup in src/gpuid.cpp. */
+int owl_device_count(int* count);
+int owl_device_info(int ordinal, char* name, size_t name_len, size_t* total_mem, char* pci_bus_id, size_t pci_len);
+
+/* FFT choice -- reference FFTConfig::bestFit (src/FFTConfig.cpp:235-263): the smallest
+   supported N = 2*W*H (W, H powers of two in [64, 4096]) with E/N <= max_bpw
+   (max_bpw <= 0 selects the default limit). */
+int owl_fft_choose(uint32_t E, double max_bpw, uint32_t* N, uint32_t* W, uint32_t* H);
+
+/* Plan = one exponent on one device with its tables and work buffers -- the reference's
+   Gpu constructor (src/Gpu.cpp:394-564: clDefines, genWeights, trig tables, buffers).
+   W = H = 0 picks the shape with owl_fft_choose(E, 0). */
+int owl_plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out);
+int owl_plan_destroy(owl_plan* plan);
+int owl_plan_shape(const owl_plan* plan, uint32_t* N, uint32_t* W, uint32_t* H);
+/* limit of every device-side wait, in nanoseconds (default 2 s) */
+int owl_plan_set_timeout(owl_plan* plan, uint64_t ns);
+
+/* Word buffers -- Buffer<int> (src/Buffer.h:16-102), AllocTrac accounting aside. */
+int owl_buf_alloc(owl_plan* plan, int32_t** buf);
+int owl_buf_free(owl_plan* plan, int32_t* buf);
+/* dst := src (operator<<, src/Buffer.h) */
+int owl_buf_copy(owl_plan* plan, int32_t* dst, const int32_t* src);
+/* buf := small integer value (Buffer::set, used by exponentiate for exp == 0) */
+int owl_buf_set(owl_plan* plan, int32_t* buf, uint32_t value);
+
+/* Raw digit transfer (N int32). */
+int owl_write_digits(owl_plan* plan, int32_t* buf, const int32_t* host);
+int owl_read_digits(owl_plan* plan, const int32_t* buf, int32_t* host);
+/* Compact words: Gpu::writeIn (expandBits, src/Gpu.cpp:801-811, src/state.cpp:93-115) and
+   Gpu::readAndCompress (readChecked + compactBits, src/Gpu.cpp:677-710). The read is
+   verified with a device-side 64-bit sum and retried up to 3 times. */
+int owl_write_words(owl_plan* plan, int32_t* buf, const uint32_t* words);
+int owl_read_words(owl_plan* plan, const int32_t* buf, uint32_t* words);
+
+/* Gpu::squareLoop(out, in, 0, n, flags & MUL3) (src/Gpu.cpp:936-945) with Gpu::square's
+   kernel chain (src/Gpu.cpp:903-932): n squarings of `in` into `out` (out may equal in).
+   OWL_SQ_LL makes every step x^2 - 2 (squareLL). */
+int owl_square(owl_plan* plan, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags);
+/* Gpu::modMul(ioA, inB, mul3) (src/Gpu.cpp:712-736): ioA := ioA * inB (* 3). */
+int owl_modmul(owl_plan* plan, int32_t* io_a, const int32_t* in_b, int mul3);
+/* Gpu::isEqual (src/Gpu.cpp:947-953, src/cl/etc.cl:34-41): digit-wise equality. */
+int owl_is_equal(owl_plan* plan, const int32_t* a, const int32_t* b, int* equal);
+/* Gpu::bufResidue (src/Gpu.cpp:955-975): res64 from the words around the wrap; falls
+   back to the full compact form when the top 32 words cannot decide the carry. */
+int owl_res64(owl_plan* plan, const int32_t* buf, uint64_t* res64);
+/* sum64 kernel (src/cl/etc.cl:19-29): the buffer as N/2 u64, summed mod 2^64. */
+int owl_sum64(owl_plan* plan, const int32_t* buf, uint64_t* sum);
+/* Gpu::readROE (src/Gpu.cpp:624-637): per-squaring max |x - rint(x)| recorded since the
+   last call (at most cap values; *n gets the count), then cleared. */
+int owl_read_roe(owl_plan* plan, float* out, uint32_t cap, uint32_t* n);
+/* wait for the plan's stream; reports a device-side wait timeout as OWL_ERR_TIMEOUT */
+int owl_sync(owl_plan* plan);
+
+/* The plan's CUDA stream (a cudaStream_t), so that callers can order their own work and
+   record CUDA events on the stream the engine's kernels run on. */
+int owl_plan_stream(owl_plan* plan, void** stream);
+
+/* Per-kernel timing of n squarings of buf (in place), the counterpart of the reference's
+   -time profile (src/Gpu.cpp:773-799, src/Queue.cpp:54-58): CUDA events bracket every launch.
+   ms[0] = total pass-2 (column) time, ms[1] = total pass-1 (line/carry) time, ms[2] = total
+   of the block's entry/exit launches; launches[0..2] the matching launch counts. */
+int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint32_t* launches);
+
+/* Failure-detection probe: one device wait on a flag nothing sets, with the plan's
+   timeout. Returns OWL_ERR_TIMEOUT (the expected outcome) and leaves the plan usable. */
+int owl_probe_wait_timeout(owl_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,209 @@
+// emu_main.cpp -- runs libowl's kernels on the CPU (owl_emu_rt.hpp) with the
+// same launch sequence as owl_square / owl_modmul, and prints the result as
+// compact words so that tests/test_emulator.py can compare it with GMP.
+//
+// TEST INFRASTRUCTURE ONLY. Usage:
+//   owl_emu square E W H n flags seed   (seed 0: start from 3, or 4 with LL)
+//   owl_emu modmul E W H mul3 seedA seedB
+// Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
+#define OWL_EMU 1
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+#include "owl_kernels.cuh"
+#include "owl_tables.hpp"
+#include "owl_words.hpp"
+
+using namespace owl;
+
+namespace {
+
+constexpr int kR = 2;
+
+struct EmuPlan {
+  Tables t;
+  Args a{};
+  std::vector<C> twW, twH, twLo, twHi, F1, F2;
+  std::vector<long long> shuttle;
+  std::vector<uint32_t> flags;
+  Ctl ctl{};
+  std::vector<float> roe;
+  int roePos = 0;
+};
+
+std::vector<C> toC(const std::vector<HostC>& v) {
+  std::vector<C> r(v.size());
+  for (size_t i = 0; i < v.size(); ++i) { r[i] = make_double2(v[i].x, v[i].y); }
+  return r;
+}
+
+void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
+  p.t = make_tables(E, W, H);
+  p.twW = toC(p.t.twW);
+  p.twH = toC(p.t.twH);
+  p.twLo = toC(p.t.twLo);
+  p.twHi = toC(p.t.twHi);
+  p.F1.assign(p.t.hN, make_double2(0, 0));
+  p.F2.assign(p.t.hN, make_double2(0, 0));
+  p.shuttle.assign((size_t)(H / kR) * W, 0);
+  p.flags.assign(H / kR, 0);
+  p.roe.assign(4096, 0.0f);
+  Args& a = p.a;
+  a.twW = p.twW.data();
+  a.twH = p.twH.data();
+  a.twLo = p.twLo.data();
+  a.twHi = p.twHi.data();
+  a.wt1 = p.t.wt1.data();
+  a.iwt1 = p.t.iwt1.data();
+  a.x1 = p.t.x1.data();
+  a.wt2 = p.t.wt2.data();
+  a.iwt2 = p.t.iwt2.data();
+  a.x2 = p.t.x2.data();
+  a.shuttle = p.shuttle.data();
+  a.flags = p.flags.data();
+  a.ctl = &p.ctl;
+  a.roe = p.roe.data();
+  a.E = E;
+  a.N = p.t.N;
+  a.W = W;
+  a.H = H;
+  a.hN = p.t.hN;
+  a.bitsLo = E / p.t.N;
+  a.eModN = E % p.t.N;
+  a.loShift = p.t.loShift;
+  a.timeoutNs = 60ull * 1000000000ull;
+}
+
+template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int flags) {
+  constexpr int T = kR * W / 16;
+  size_t sm = (size_t)kR * p1_line_stride<W, kR>() * sizeof(C);
+  Args a = p.a;
+  emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M>(a, F, words, slot, flags); });
+}
+template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {
+  constexpr int T = H / 8;
+  size_t sm = 2 * (size_t)p2_col_stride<H>() * sizeof(C);
+  Args a = p.a;
+  emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M>(a, F, Fb, Fq); });
+}
+
+template <int W> void p1w(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {
+  int slot = -1;
+  if (mode != P1_IN) { slot = p.roePos++; }
+  if (mode == P1_FUSED) p1m<W, P1_FUSED>(p, F, words, slot, flags);
+  else if (mode == P1_IN) p1m<W, P1_IN>(p, F, words, slot, flags);
+  else p1m<W, P1_OUT>(p, F, words, slot, flags);
+}
+template <int H> void p2h(EmuPlan& p, int mode, C* F, const C* Fb, C* Fq) {
+  if (mode == P2_SQUARE) p2m<H, P2_SQUARE>(p, F, Fb, Fq);
+  else if (mode == P2_FWD) p2m<H, P2_FWD>(p, F, Fb, Fq);
+  else p2m<H, P2_MUL>(p, F, Fb, Fq);
+}
+
+void pass1(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {
+  switch (p.t.W) {
+    case 64: p1w<64>(p, mode, F, words, flags); break;
+    case 128: p1w<128>(p, mode, F, words, flags); break;
+    case 256: p1w<256>(p, mode, F, words, flags); break;
+    default: throw std::runtime_error("emu W");
+  }
+  if (p.ctl.error) { throw std::runtime_error("device wait timeout in emulation"); }
+}
+void pass2(EmuPlan& p, int mode, C* F, const C* Fb, C* Fq) {
+  switch (p.t.H) {
+    case 64: p2h<64>(p, mode, F, Fb, Fq); break;
+    case 128: p2h<128>(p, mode, F, Fb, Fq); break;
+    case 256: p2h<256>(p, mode, F, Fb, Fq); break;
+    case 512: p2h<512>(p, mode, F, Fb, Fq); break;
+    default: throw std::runtime_error("emu H");
+  }
+}
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+std::vector<uint32_t> start_words(uint32_t E, uint64_t seed, uint32_t small) {
+  std::vector<uint32_t> w(n_words(E), 0);
+  if (seed == 0) {
+    w[0] = small;
+    return w;
+  }
+  uint64_t s = seed;
+  for (auto& x : w) { x = (uint32_t)splitmix(s); }
+  uint32_t top = E % 32;
+  if (top) { w.back() &= (1u << top) - 1; }
+  return w;
+}
+
+void print_words(const std::vector<int32_t>& d, uint32_t N, uint32_t E, float roe) {
+  std::vector<uint32_t> out(n_words(E));
+  if (!compact_bits(d.data(), N, E, out.data())) {
+    std::printf("error compact\n");
+    std::exit(3);
+  }
+  std::printf("roe %.6f\n", roe);
+  for (size_t i = 0; i < out.size(); ++i) { std::printf("%08x%c", out[i], i + 1 == out.size() ? '\n' : ' '); }
+}
+
+float max_roe(const EmuPlan& p) {
+  float m = 0;
+  for (int i = 0; i < p.roePos; ++i) { m = std::max(m, p.roe[i]); }
+  return m;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 2) { return 2; }
+  std::string mode = argv[1];
+  try {
+    if (mode == "square" && argc == 8) {
+      uint32_t E = std::strtoul(argv[2], nullptr, 10), W = std::strtoul(argv[3], nullptr, 10),
+               H = std::strtoul(argv[4], nullptr, 10), n = std::strtoul(argv[5], nullptr, 10),
+               flags = std::strtoul(argv[6], nullptr, 10);
+      uint64_t seed = std::strtoull(argv[7], nullptr, 10);
+      EmuPlan p;
+      init(p, E, W, H);
+      const uint32_t N = p.t.N;
+      auto w = start_words(E, seed, (flags & FL_LL) ? 4 : 3);
+      std::vector<int32_t> in(N), out(N);
+      if (!expand_bits(w.data(), N, E, in.data())) { return 3; }
+      pass1(p, P1_IN, p.F1.data(), in.data(), 0);
+      for (uint32_t k = 0; k < n; ++k) {
+        pass2(p, P2_SQUARE, p.F1.data(), nullptr, nullptr);
+        if (k + 1 < n) pass1(p, P1_FUSED, p.F1.data(), nullptr, flags & FL_LL);
+        else pass1(p, P1_OUT, p.F1.data(), out.data(), flags);
+      }
+      print_words(out, N, E, max_roe(p));
+      return 0;
+    }
+    if (mode == "modmul" && argc == 8) {
+      uint32_t E = std::strtoul(argv[2], nullptr, 10), W = std::strtoul(argv[3], nullptr, 10),
+               H = std::strtoul(argv[4], nullptr, 10), mul3 = std::strtoul(argv[5], nullptr, 10);
+      uint64_t sa = std::strtoull(argv[6], nullptr, 10), sb = std::strtoull(argv[7], nullptr, 10);
+      EmuPlan p;
+      init(p, E, W, H);
+      const uint32_t N = p.t.N;
+      auto wa = start_words(E, sa, 3), wb = start_words(E, sb, 3);
+      std::vector<int32_t> a(N), b(N);
+      if (!expand_bits(wa.data(), N, E, a.data()) || !expand_bits(wb.data(), N, E, b.data())) { return 3; }
+      pass1(p, P1_IN, p.F2.data(), b.data(), 0);
+      pass2(p, P2_FWD, p.F2.data(), nullptr, p.F2.data());
+      pass1(p, P1_IN, p.F1.data(), a.data(), 0);
+      pass2(p, P2_MUL, p.F1.data(), p.F2.data(), nullptr);
+      pass1(p, P1_OUT, p.F1.data(), a.data(), mul3 ? FL_MUL3 : 0);
+      print_words(a, N, E, max_roe(p));
+      return 0;
+    }
+  } catch (const std::exception& e) {
+    std::printf("error %s\n", e.what());
+    return 4;
+  }
+  return 2;
+}

@@ -1,0 +1,70 @@
+"""The C ABI (include/owl.h): the library builds for sm_100a, loads without a GPU, exports every
+declared entry point, and its no-device paths fail cleanly."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "owl.h")
+
+
+def declared():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*|void)\s+(owl_\w+)\s*\(", src, re.M)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from gpuowl_b200 import build
+    build.build()
+    import gpuowl_b200 as g
+    return g.load()
+
+
+def test_header_declares_the_boundary():
+    names = declared()
+    for must in ("owl_plan_create", "owl_square", "owl_modmul", "owl_res64", "owl_read_words",
+                 "owl_write_words", "owl_is_equal", "owl_read_roe", "owl_probe_wait_timeout"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", os.path.join(ROOT, "gpuowl_b200", "libowl.so")],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\sT\s+(owl_\w+)$", out, re.M))
+    missing = [n for n in declared() if n not in exported]
+    assert not missing, missing
+
+
+def test_build_targets_sm100a_only():
+    from gpuowl_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_abi_version_and_errors(lib):
+    assert lib.owl_abi_version() == 1
+    assert lib.owl_error_string(-4) == b"device wait timeout"
+    # null / bogus arguments fail with a status, never a crash
+    assert lib.owl_plan_destroy(None) == -1
+    assert lib.owl_square(None, None, None, 1, 0) == -1
+
+
+def test_fft_choice_matches_the_configs(lib):
+    import gpuowl_b200 as g
+    assert g.fft_choose(4989349) == (262144, 256, 512)        # 256K (reference 256:2:256)
+    assert g.fft_choose(136181029) == (8388608, 2048, 2048)   # 8M  (reference 1K:8:512)
+    with pytest.raises(g.OwlError):
+        g.fft_choose(3_000_000_000)
+
+
+def test_plan_without_device_reports_nodev(lib):
+    import gpuowl_b200 as g
+    if g.device_count() > 0:
+        pytest.skip("a device is present")
+    with pytest.raises(g.OwlError) as e:
+        g.Plan(86243)
+    assert e.value.status == -5

@@ -1,0 +1,188 @@
+"""GPU parity: libowl (through the C ABI) against the GMP oracle and the golden res64 tables.
+
+Bar: bit-exact integers -- identical compact words / res64 -- for every case.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, random_words, res64_of, small_words
+
+pytestmark = pytest.mark.gpu
+
+# (E, W, H): every pass-1 / pass-2 instantiation from 8K to 8M words, at 10.5 .. 19 bits/word
+SHAPES = [
+    (86243, 64, 64), (216091, 64, 128), (500009, 128, 128), (1000003, 128, 256),
+    (1999993, 256, 256), (4989349, 256, 512), (9000011, 512, 512), (17000023, 512, 1024),
+    (33000001, 1024, 1024), (66000001, 1024, 2048), (136181029, 2048, 2048),
+]
+
+
+@pytest.mark.parametrize("E,W,H", SHAPES[:7])
+@pytest.mark.parametrize("ll", [False, True])
+def test_square_random_vs_gmp(owl, oracle, E, W, H, ll):
+    """n squarings of a random residue equal GMP's, word for word."""
+    n = 20
+    with owl.Plan(E, W=W, H=H) as p:
+        start = random_words(E, E * 7 + 1)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.squareLoop(a, a, n, ll=ll)
+        got = p.readOut(a)
+    want = oracle.gmp_square(E, start, n, ll=ll)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("E,W,H", SHAPES[7:])
+def test_square_large_shapes_vs_gmp(owl, oracle, E, W, H):
+    n = 6
+    with owl.Plan(E, W=W, H=H) as p:
+        start = random_words(E, E + 3)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.squareLoop(a, a, n)
+        got = p.readOut(a)
+    want = oracle.gmp_square(E, start, n)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("E,W,H", [SHAPES[0], SHAPES[3], SHAPES[5], SHAPES[8]])
+def test_mul3_last(owl, oracle, E, W, H):
+    """squareLoop with doTailMul3: the last squaring is multiplied by 3 (Gerbicz aux)."""
+    n = 7
+    with owl.Plan(E, W=W, H=H) as p:
+        start = random_words(E, 99)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.squareLoop(a, a, n, mul3=True)
+        got = p.readOut(a)
+    want = oracle.gmp_mul(E, oracle.gmp_square(E, start, n), small_words(E, 3))
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("E,W,H", [SHAPES[0], SHAPES[2], SHAPES[5], SHAPES[8], SHAPES[10]])
+@pytest.mark.parametrize("mul3", [False, True])
+def test_modmul_vs_gmp(owl, oracle, E, W, H, mul3):
+    with owl.Plan(E, W=W, H=H) as p:
+        wa, wb = random_words(E, 5), random_words(E, 6)
+        a, b = p.alloc(), p.alloc()
+        p.writeIn(a, wa)
+        p.writeIn(b, wb)
+        p.modMul(a, b, mul3=mul3)
+        got = p.readOut(a)
+        # the second operand is untouched
+        assert np.array_equal(p.readOut(b), oracle.gmp_square(E, wb, 0))
+    assert np.array_equal(got, oracle.gmp_mul(E, wa, wb, mul3=mul3))
+
+
+def test_write_read_roundtrip_and_res64(owl, oracle):
+    E = 4989349
+    with owl.Plan(E) as p:
+        w = random_words(E, 1234)
+        a = p.alloc()
+        p.writeIn(a, w)
+        assert np.array_equal(p.readOut(a), w)
+        assert p.bufResidue(a) == res64_of(w)
+        # digits agree with the oracle's expandBits
+        assert np.array_equal(p.read_digits(a), oracle.expand(E, p.N, w))
+        p.squareLoop(a, a, 3)
+        out = p.readOut(a)
+        assert p.bufResidue(a) == res64_of(out)
+
+
+def test_is_equal_and_sum64(owl):
+    E = 216091
+    with owl.Plan(E) as p:
+        a, b = p.alloc(), p.alloc()
+        w = random_words(E, 77)
+        p.writeIn(a, w)
+        p.copy(b, a)
+        assert p.isEqual(a, b)
+        d = p.read_digits(a)
+        d[12345 % p.N] += 1
+        p.write_digits(b, d)
+        assert not p.isEqual(a, b)
+        want = int(np.ascontiguousarray(p.read_digits(a)).view(np.uint64).sum(dtype=np.uint64))
+        assert p.sum64(a) == want
+
+
+@pytest.mark.parametrize("E", [86243, 110503, 132049])
+def test_mersenne_prime_prp_is_9(owl, E):
+    """M_E prime: 3^(2^E) = 9 mod M_E (the reference's equals9, src/Gpu.cpp:1036-1040)."""
+    with owl.Plan(E) as p:
+        a = p.alloc()
+        p.writeIn(a, small_words(E, 3))
+        p.squareLoop(a, a, E)
+        w = p.readOut(a)
+    assert w[0] == 9 and not w[1:].any()
+
+
+@pytest.mark.parametrize("E", [86243, 132049])
+def test_mersenne_prime_ll_is_0(owl, E):
+    """M_E prime: the LL sequence from 4 reaches 0 after E-2 steps."""
+    with owl.Plan(E) as p:
+        a = p.alloc()
+        p.writeIn(a, small_words(E, 4))
+        p.squareLoop(a, a, E - 2, ll=True)
+        w = p.readOut(a)
+    # 0 mod M_E may come back as 0 or as M_E itself (all ones)
+    full = np.full_like(w, 0xFFFFFFFF)
+    if E % 32:
+        full[-1] = (1 << (E % 32)) - 1
+    assert not w.any() or np.array_equal(w, full)
+
+
+def _run_golden(owl, item, shape=None):
+    E, step, iters = item["E"], item["step"], item["iters"]
+    ll = item["kind"] == "ll"
+    kw = {} if shape is None else dict(W=shape[0], H=shape[1])
+    with owl.Plan(E, **kw) as p:
+        a = p.alloc()
+        p.writeIn(a, small_words(E, item["start"]))
+        got = []
+        for _ in range(iters // step):
+            p.squareLoop(a, a, step, ll=ll)
+            got.append("%016x" % p.bufResidue(a))
+        roe = p.readROE()
+    return got, float(roe.max()) if roe.size else 0.0
+
+
+def test_golden_small(owl):
+    g = load_golden("small")
+    for item in g["items"]:
+        if item["E"] < 65536:
+            continue  # below the smallest FFT (N = 8K at <= 19 bits/word is fine, but 2 bits/word is not)
+        got, roe = _run_golden(owl, item)
+        assert got == item["res64"], item["E"]
+        assert roe < 0.3
+
+
+def test_golden_prp_256k(owl):
+    """PRP-3 at 256K, E from seed in [4.8M, 5.0M] (19.03 bits/word), 20,000 iterations."""
+    g = load_golden("prp_256k")
+    got, roe = _run_golden(owl, g)
+    assert got == g["res64"]
+    assert roe < 0.45
+
+
+@pytest.mark.parametrize("name", ["prp_8m", "ll_8m"])
+def test_golden_8m(owl, name):
+    """8M FFT (W=H=2048), E from seed in [136M, 139M], 10,000 iterations: res64 every 1,000,
+    and the max round-off stays within the 0.35 bound."""
+    g = load_golden(name)
+    got, roe = _run_golden(owl, g, shape=(2048, 2048))
+    assert got == g["res64"]
+    assert roe <= 0.35
+
+
+def test_wait_timeout_probe_keeps_plan_usable(owl, oracle):
+    """A device wait that nothing ends returns OWL_ERR_TIMEOUT; the plan then still computes."""
+    E = 86243
+    with owl.Plan(E) as p:
+        p.set_timeout(5_000_000)  # 5 ms
+        assert p.probe_wait_timeout() == owl.ERR_TIMEOUT
+        p.set_timeout(2_000_000_000)
+        a = p.alloc()
+        w = random_words(E, 3)
+        p.writeIn(a, w)
+        p.squareLoop(a, a, 5)
+        assert np.array_equal(p.readOut(a), oracle.gmp_square(E, w, 5))
