@@ -202,6 +202,13 @@ void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq) {
   ck(cudaGetLastError(), "pass2 launch");
 }
 
+// the block-exit line pass, then the (normally empty) queue of leftover carries
+void pass1_out(owl_plan* p, int32_t* words, int flags) {
+  pass1(p, owl::P1_OUT, p->F1, words, flags);
+  owl::k_carry_fixup<<<1, 32, 0, p->stream>>>(p->args, words);
+  ck(cudaGetLastError(), "fixup launch");
+}
+
 void check_plan(const owl_plan* p) {
   if (!p) { fail(OWL_ERR_ARG, "null plan"); }
 }
@@ -299,7 +306,8 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
 
   // scratch: carry shuttle, flags, control word, ROE slots, small outputs
   const uint32_t G = H / kR;
-  size_t sbytes = 256 * 8 + (size_t)G * W * sizeof(long long) + G * sizeof(uint32_t) + sizeof(owl::Ctl) +
+  size_t sbytes = 256 * 9 + (size_t)G * W * sizeof(long long) + G * sizeof(uint32_t) + sizeof(owl::Ctl) +
+                  2 * owl::kPendingCap * sizeof(long long) +
                   kRoeCap * sizeof(float) + 64 * sizeof(int32_t) + sizeof(unsigned long long) + sizeof(int);
   ck(cudaMalloc(&p->scratch, sbytes), "cudaMalloc(scratch)");
   ck(cudaMemset(p->scratch, 0, sbytes), "memset(scratch)");
@@ -307,6 +315,7 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   p->args.shuttle = carve<long long>(cur, (size_t)G * W);
   p->args.flags = carve<uint32_t>(cur, G);
   p->args.ctl = carve<owl::Ctl>(cur, 1);
+  p->args.pending = carve<long long>(cur, 2 * owl::kPendingCap);
   p->args.roe = carve<float>(cur, kRoeCap);
   p->small = carve<int32_t>(cur, 64);
   p->sum = carve<unsigned long long>(cur, 1);
@@ -565,7 +574,7 @@ int owl_square(owl_plan* plan, int32_t* out, const int32_t* in, uint32_t n, uint
       if (k + 1 < n) {
         pass1(plan, owl::P1_FUSED, plan->F1, nullptr, ll);
       } else {
-        pass1(plan, owl::P1_OUT, plan->F1, out, ll | mul3);
+        pass1_out(plan, out, ll | mul3);
       }
     }
   });
@@ -581,7 +590,7 @@ int owl_modmul(owl_plan* plan, int32_t* io_a, const int32_t* in_b, int mul3) {
     pass2(plan, owl::P2_FWD, plan->F2, nullptr, plan->F2);
     pass1(plan, owl::P1_IN, plan->F1, io_a, 0);
     pass2(plan, owl::P2_MUL, plan->F1, plan->F2, nullptr);
-    pass1(plan, owl::P1_OUT, plan->F1, io_a, mul3 ? owl::FL_MUL3 : 0);
+    pass1_out(plan, io_a, mul3 ? owl::FL_MUL3 : 0);
   });
 }
 
@@ -701,7 +710,7 @@ int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint
       if (k + 1 < n) {
         pass1(plan, owl::P1_FUSED, plan->F1, nullptr, 0);
       } else {
-        pass1(plan, owl::P1_OUT, plan->F1, buf, 0);
+        pass1_out(plan, buf, 0);
       }
       ck(cudaEventRecord(ev[3 + 2 * k], plan->stream), "record");
     }
@@ -720,7 +729,7 @@ int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint
     ms[2] = te;
     launches[0] = n;
     launches[1] = n - 1;
-    launches[2] = 2;
+    launches[2] = 3;
   });
 }
 

@@ -27,12 +27,14 @@
 namespace owl {
 
 struct Ctl {
-  uint32_t ticket;  // line-group ticket for the carry chain (reset by the last taker)
-  uint32_t error;   // OWL_DEVERR_* bits, sticky until the host clears them
-  uint32_t pad[30];
+  uint32_t ticket;    // line-group ticket for the carry chain (reset by the last taker)
+  uint32_t error;     // DEVERR_* bits, sticky until the host clears them
+  uint32_t npending;  // carries left over at the end of a thread's word chain (block exit only)
+  uint32_t pad[29];
 };
 
-enum : uint32_t { DEVERR_WAIT = 1u };
+enum : uint32_t { DEVERR_WAIT = 1u, DEVERR_PENDING = 2u };
+constexpr uint32_t kPendingCap = 1024;
 
 struct Args {
   const C* twW;    // w_W^i, i < W
@@ -46,6 +48,7 @@ struct Args {
   const double* iwt2;  // per (line j2, e): 2^(-X2/N) / (4 hN)
   const uint32_t* x2;  // per (line j2, e): X2 = step*(2 j2 + e) mod N
   long long* shuttle;  // carry rows, (H/R) x W
+  long long* pending;  // (word index, carry) pairs, kPendingCap entries
   uint32_t* flags;     // per line group
   Ctl* ctl;
   float* roe;          // per-launch max round-off slots
@@ -267,18 +270,48 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
       }
     }
     __syncthreads();
-    // carry-in for line 0 of this group (carryFinal, src/cl/carryinc.cl:18-23)
+    // carry-in for line 0 of this group
     const uint32_t prevg = (g == 0) ? G - 1 : g - 1;
 #pragma unroll
     for (int r = 0; r < RL; ++r) {
       const uint32_t j1 = t + (W / RL) * r;
       uint32_t src = (g == 0) ? (j1 == 0 ? W - 1 : j1 - 1) : j1;
       long long cin = __ldcg(a.shuttle + (size_t)prevg * W + src);
-      uint32_t bits0 = a.bitsLo + ((bigmask >> ((r * R + 0) * 2 + 0)) & 1u);
-      long long xx = dig[0][r][0] + cin;
-      long long dd = sext_low(xx, bits0);
-      dig[0][r][0] = dd;
-      dig[0][r][1] += (xx - dd) >> bits0;
+      if constexpr (MODE == P1_FUSED) {
+        // sloppy: two words only, the digits feed the next FFT (carryFinal,
+        // src/cl/carryinc.cl:18-23)
+        uint32_t bits0 = a.bitsLo + ((bigmask >> ((r * R + 0) * 2 + 0)) & 1u);
+        long long xx = dig[0][r][0] + cin;
+        long long dd = sext_low(xx, bits0);
+        dig[0][r][0] = dd;
+        dig[0][r][1] += (xx - dd) >> bits0;
+      } else {
+        // block exit: propagate through the thread's whole chain so that every
+        // digit is balanced -- the canonical form isEqual compares (carryB,
+        // src/cl/carryb.cl:5-32); a carry that survives the chain is queued
+        long long c = cin;
+#pragma unroll
+        for (int ll = 0; ll < R; ++ll) {
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            uint32_t bits = a.bitsLo + ((bigmask >> ((r * R + ll) * 2 + e)) & 1u);
+            long long xx = dig[ll][r][e] + c;
+            long long dd = sext_low(xx, bits);
+            c = (xx - dd) >> bits;
+            dig[ll][r][e] = dd;
+          }
+        }
+        if (c != 0) {
+          uint32_t i = atomicAdd(&a.ctl->npending, 1u);
+          if (i < kPendingCap) {
+            uint64_t next = 2ull * ((uint64_t)a.H * j1 + g * R + R);
+            a.pending[2 * i] = (long long)(next % a.N);
+            a.pending[2 * i + 1] = c;
+          } else {
+            atomicOr(&a.ctl->error, DEVERR_PENDING);
+          }
+        }
+      }
     }
   }
 
@@ -614,6 +647,29 @@ __global__ void k_sum64(const unsigned long long* __restrict__ in, size_t n64, u
 __global__ void k_gather_residue(const int32_t* __restrict__ data, uint32_t N, int32_t* out) {
   int i = threadIdx.x;
   if (i < 64) { out[i] = data[(N - 32 + i) % N]; }
+}
+
+// Applies the carries queued by a block-exit line pass, one after the other,
+// each propagated word by word (with wrap-around) until it is absorbed.
+__global__ void k_carry_fixup(Args a, int32_t* __restrict__ words) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) { return; }
+  uint32_t n = a.ctl->npending;
+  if (n > kPendingCap) { n = kPendingCap; }
+  const uint64_t step = a.N - a.E % a.N;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t w = (uint32_t)a.pending[2 * i];
+    long long c = a.pending[2 * i + 1];
+    for (uint32_t k = 0; c != 0 && k < a.N; ++k) {
+      uint32_t extra = (uint32_t)((step * w) % a.N);
+      uint32_t bits = a.bitsLo + (extra < a.eModN ? 1u : 0u);
+      long long xx = (long long)words[w] + c;
+      long long dd = sext_low(xx, bits);
+      c = (xx - dd) >> bits;
+      words[w] = (int32_t)dd;
+      w = (w + 1 == a.N) ? 0 : w + 1;
+    }
+  }
+  a.ctl->npending = 0;
 }
 
 // timeout probe: wait on a flag that is never set, with the pass-1 wait loop

@@ -26,7 +26,7 @@ struct EmuPlan {
   Tables t;
   Args a{};
   std::vector<C> twW, twH, twLo, twHi, F1, F2;
-  std::vector<long long> shuttle;
+  std::vector<long long> shuttle, pending;
   std::vector<uint32_t> flags;
   Ctl ctl{};
   std::vector<float> roe;
@@ -48,6 +48,7 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   p.F1.assign(p.t.hN, make_double2(0, 0));
   p.F2.assign(p.t.hN, make_double2(0, 0));
   p.shuttle.assign((size_t)(H / kR) * W, 0);
+  p.pending.assign(2 * kPendingCap, 0);
   p.flags.assign(H / kR, 0);
   p.roe.assign(4096, 0.0f);
   Args& a = p.a;
@@ -62,6 +63,7 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   a.iwt2 = p.t.iwt2.data();
   a.x2 = p.t.x2.data();
   a.shuttle = p.shuttle.data();
+  a.pending = p.pending.data();
   a.flags = p.flags.data();
   a.ctl = &p.ctl;
   a.roe = p.roe.data();
@@ -109,6 +111,10 @@ void pass1(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {
     case 256: p1w<256>(p, mode, F, words, flags); break;
     default: throw std::runtime_error("emu W");
   }
+  if (mode == P1_OUT) {
+    Args a = p.a;
+    emu_launch(1, 32, 0, [=] { k_carry_fixup(a, words); });
+  }
   if (p.ctl.error) { throw std::runtime_error("device wait timeout in emulation"); }
 }
 void pass2(EmuPlan& p, int mode, C* F, const C* Fb, C* Fq) {
@@ -142,6 +148,14 @@ std::vector<uint32_t> start_words(uint32_t E, uint64_t seed, uint32_t small) {
 }
 
 void print_words(const std::vector<int32_t>& d, uint32_t N, uint32_t E, float roe) {
+  // every digit of a block-exit buffer must be balanced: -2^(b-1) <= d < 2^(b-1)
+  for (uint32_t k = 0; k < N; ++k) {
+    int32_t half = 1 << (word_bits(N, E, k) - 1);
+    if (d[k] < -half || d[k] >= half) {
+      std::printf("error unbalanced digit %u\n", k);
+      std::exit(5);
+    }
+  }
   std::vector<uint32_t> out(n_words(E));
   if (!compact_bits(d.data(), N, E, out.data())) {
     std::printf("error compact\n");

@@ -186,3 +186,30 @@ def test_wait_timeout_probe_keeps_plan_usable(owl, oracle):
         p.writeIn(a, w)
         p.squareLoop(a, a, 5)
         assert np.array_equal(p.readOut(a), oracle.gmp_square(E, w, 5))
+
+
+@pytest.mark.parametrize("E", [216091, 4989349])
+def test_gerbicz_identity_and_injected_fault(owl, E):
+    """Reference PRP loop + doCheck (src/Gpu.cpp:738-771): after blocks of
+    check *= data; data <- data^(2^B), the identity check^(2^B) * 3 == check * data
+    holds and isEqual sees it on the digits; one flipped word in data breaks it."""
+    B = 40
+    with owl.Plan(E) as p:
+        data, check, aux = p.alloc(), p.alloc(), p.alloc()
+        p.writeIn(data, small_words(E, 3))
+        p.writeIn(check, small_words(E, 1))
+        for _ in range(3):
+            p.modMul(check, data)
+            p.squareLoop(data, data, B)
+        saved = p.alloc()
+        p.copy(saved, check)
+        p.squareLoop(aux, check, B, mul3=True)
+        p.modMul(check, data)
+        assert p.isEqual(check, aux)
+        # fault injected on the host between blocks: the check must fail
+        d = p.read_digits(data)
+        d[777] ^= 1
+        p.write_digits(data, d)
+        p.copy(check, saved)
+        p.modMul(check, data)
+        assert not p.isEqual(check, aux)
