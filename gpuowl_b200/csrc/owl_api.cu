@@ -275,8 +275,9 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   ck(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "cudaStreamCreate");
 
   // tables: one allocation
-  size_t nC = t.twW.size() + t.twH.size() + t.twLo.size() + t.twHi.size();
-  size_t bytes = 256 * 12 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
+  static_assert(kR == owl::kLinesPerBlock, "table layout and launch disagree on lines per block");
+  size_t nC = t.twW.size() + t.twH.size() + t.rootH.size() + t.twLo.size() + t.twHi.size();
+  size_t bytes = 256 * 13 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
                  (t.x1.size() + t.x2.size()) * sizeof(uint32_t);
   ck(cudaMalloc(&p->tableMem, bytes), "cudaMalloc(tables)");
   std::vector<char> host(bytes, 0);
@@ -290,6 +291,7 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   char* dbase = static_cast<char*>(p->tableMem);
   p->args.twW = reinterpret_cast<const C*>(dbase + put(t.twW.data(), t.twW.size() * sizeof(C)));
   p->args.twH = reinterpret_cast<const C*>(dbase + put(t.twH.data(), t.twH.size() * sizeof(C)));
+  p->args.rootH = reinterpret_cast<const C*>(dbase + put(t.rootH.data(), t.rootH.size() * sizeof(C)));
   p->args.twLo = reinterpret_cast<const C*>(dbase + put(t.twLo.data(), t.twLo.size() * sizeof(C)));
   p->args.twHi = reinterpret_cast<const C*>(dbase + put(t.twHi.data(), t.twHi.size() * sizeof(C)));
   p->args.wt1 = reinterpret_cast<const double*>(dbase + put(t.wt1.data(), t.wt1.size() * sizeof(double)));

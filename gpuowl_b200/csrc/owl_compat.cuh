@@ -28,5 +28,26 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 __device__ __forceinline__ void spin_pause() { __nanosleep(20); }
+
+// The FFT state is streamed through L1 without allocating (so that the twiddle
+// and weight tables stay resident) and kept in L2 with evict-last priority: at
+// 8M words the 64 MiB state fits in the 126 MB L2 between the two passes.
+__device__ __forceinline__ unsigned long long l2_keep_policy() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ double2 ld_state(const double2* ptr, unsigned long long pol) {
+  double2 v;
+  asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+               : "=d"(v.x), "=d"(v.y)
+               : "l"(ptr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_state(double2* ptr, double2 v, unsigned long long pol) {
+  asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(ptr), "d"(v.x), "d"(v.y),
+               "l"(pol)
+               : "memory");
+}
 }  // namespace owl
 #endif

@@ -82,6 +82,20 @@ template <bool INV, int M> __device__ __forceinline__ C mul_w16(C a) {
   }
 }
 
+// a * w8^r for r known after unrolling
+template <bool INV> __device__ __forceinline__ C mul_w8(C a, int r) {
+  switch (r & 7) {
+    case 0: return a;
+    case 1: return mul_w16<INV, 2>(a);
+    case 2: return mul_w16<INV, 4>(a);
+    case 3: return mul_w16<INV, 6>(a);
+    case 4: return mul_w16<INV, 8>(a);
+    case 5: return mul_w16<INV, 10>(a);
+    case 6: return mul_w16<INV, 12>(a);
+    default: return mul_w16<INV, 14>(a);
+  }
+}
+
 template <bool INV> __device__ __forceinline__ void dft2(C* v) {
   C a = v[0];
   v[0] = cadd(a, v[1]);
@@ -179,7 +193,7 @@ template <int R, int N, int PS> __device__ __forceinline__ void st_load(const C*
   }
 }
 
-// tab: w_N^i for i < N (forward sign)
+// tab: this stage's [r][k] table, entry r * NS + k = w_(R NS)^(r k)
 template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twiddle(int tl, C* v, const C* __restrict__ tab) {
   if constexpr (NS > 1) {
 #pragma unroll
@@ -188,7 +202,7 @@ template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twi
       int k = j & (NS - 1);
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        C w = __ldg(tab + r * k * (N / (NS * R)));
+        C w = __ldg(tab + r * NS + k);
         v[b * R + r] = cmulw<INV>(v[b * R + r], w);
       }
     }
@@ -212,12 +226,35 @@ template <int R, int N, int NS, int PS> __device__ __forceinline__ void st_store
 
 // Radix plan for a line of N points whose last inverse / first forward stage
 // (radix RL) is split across lines or columns: N = R1 * M1 * M2 * RL.
+// "A order" runs the stages R1, M1, M2, RL; "B order" runs RL, M2, M1, R1.
+constexpr int plan_r1(int n, int rl) { return n / rl >= 16 ? 16 : n / rl; }
+constexpr int plan_m1(int n, int rl) { return (n / rl / plan_r1(n, rl)) >= 16 ? 16 : n / rl / plan_r1(n, rl); }
+constexpr int plan_m2(int n, int rl) { return n / rl / plan_r1(n, rl) / plan_m1(n, rl); }
+
+// Stage twiddle tables, one per stage with twiddles, each laid out [r][k]:
+// entry r * NS + k = w_(R NS)^(r k) (forward sign), so that a warp's threads
+// (consecutive k) read one contiguous run per r. Offsets in complex elements.
+struct TwOffsets {
+  int aM1, aM2, aRL, bM2, bM1, bR1, total;
+};
+constexpr TwOffsets tw_offsets(int n, int rl) {
+  const int r1 = plan_r1(n, rl), m1 = plan_m1(n, rl), m2 = plan_m2(n, rl);
+  TwOffsets o{};
+  o.aM1 = 0;
+  o.aM2 = o.aM1 + (m1 > 1 ? m1 * r1 : 0);
+  o.aRL = o.aM2 + (m2 > 1 ? m2 * r1 * m1 : 0);
+  o.bM2 = o.aRL + n;
+  o.bM1 = o.bM2 + (m2 > 1 ? m2 * rl : 0);
+  o.bR1 = o.bM1 + (m1 > 1 ? m1 * rl * m2 : 0);
+  o.total = o.bR1 + n;
+  return o;
+}
+
 template <int N, int RL> struct Plan {
-  static constexpr int REST = N / RL;
-  static constexpr int R1 = REST >= 16 ? 16 : REST;
-  static constexpr int REST2 = REST / R1;
-  static constexpr int M1 = REST2 >= 16 ? 16 : REST2;
-  static constexpr int M2 = REST2 / M1;
+  static constexpr int R1 = plan_r1(N, RL);
+  static constexpr int M1 = plan_m1(N, RL);
+  static constexpr int M2 = plan_m2(N, RL);
+  static constexpr TwOffsets TW = tw_offsets(N, RL);
   static_assert(R1 * M1 * M2 * RL == N, "plan");
   static_assert(M2 >= 1 && M2 <= 16, "plan depth");
   static_assert(R1 >= 4, "first radix too small for conflict-free padding");

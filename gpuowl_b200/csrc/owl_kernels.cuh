@@ -37,8 +37,9 @@ enum : uint32_t { DEVERR_WAIT = 1u, DEVERR_PENDING = 2u };
 constexpr uint32_t kPendingCap = 1024;
 
 struct Args {
-  const C* twW;    // w_W^i, i < W
-  const C* twH;    // w_H^i, i < H
+  const C* twW;    // stage tables of the width FFT (tw_offsets(W, 16/R) layout)
+  const C* twH;    // stage tables of the height FFT (tw_offsets(H, 8) layout)
+  const C* rootH;  // w_H^i, i < H
   const C* twLo;   // w_hN^i, i < 2^loShift
   const C* twHi;   // w_hN^(i << loShift)
   const double* wt1;   // per column j1: 2^(X1/N)
@@ -130,6 +131,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
     g = s_g;
   }
 
+  const unsigned long long pol = l2_keep_policy();
   // per-line mapping for the inner stages
   const int l = t % R;
   const int tl = t / R;
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
         for (int r = 0; r < P::R1; ++r) {
           uint32_t k1 = j + r * (W / P::R1), c, s;
           colpair(W, k1, c, s);
-          u[b * P::R1 + r] = F[faddr<R>(W, g * R + l, c, s)];
+          u[b * P::R1 + r] = ld_state(F + faddr<R>(W, g * R + l, c, s), pol);
         }
       }
       st_dft<P::R1, true>(u);
@@ -159,7 +161,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
       constexpr int PS_AFTER_M1 = (P::M1 > 1) ? 4 : PS_R1;
       if constexpr (P::M1 > 1) {
         st_load<P::M1, W, PS_R1>(line, tl, u);
-        st_twiddle<P::M1, W, NS2, true>(tl, u, a.twW);
+        st_twiddle<P::M1, W, NS2, true>(tl, u, a.twW + P::TW.aM1);
         st_dft<P::M1, true>(u);
         __syncthreads();
         st_store<P::M1, W, NS2, 4>(line, tl, u);
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
       constexpr int PS_AFTER_M2 = (P::M2 > 1) ? 4 : PS_AFTER_M1;
       if constexpr (P::M2 > 1) {
         st_load<P::M2, W, PS_AFTER_M1>(line, tl, u);
-        st_twiddle<P::M2, W, NS3, true>(tl, u, a.twW);
+        st_twiddle<P::M2, W, NS3, true>(tl, u, a.twW + P::TW.aM2);
         st_dft<P::M2, true>(u);
         __syncthreads();
         st_store<P::M2, W, NS3, 4>(line, tl, u);
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
         for (int r = 0; r < RL; ++r) { v[ll * RL + r] = ln[pad<PS_AFTER_M2>(t + r * NSL)]; }
         if constexpr (NSL > 1) {
 #pragma unroll
-          for (int r = 1; r < RL; ++r) { v[ll * RL + r] = cmulw<true>(v[ll * RL + r], __ldg(a.twW + r * t)); }
+          for (int r = 1; r < RL; ++r) { v[ll * RL + r] = cmulw<true>(v[ll * RL + r], __ldg(a.twW + P::TW.aRL + r * NSL + t)); }
         }
         dftR<RL, true>(v + ll * RL);
       }
@@ -364,7 +366,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
     constexpr int PS_A = (P::M2 > 1) ? 4 : PS_RL;
     if constexpr (P::M2 > 1) {
       st_load<P::M2, W, PS_RL>(line, tl, u);
-      st_twiddle<P::M2, W, NSa, false>(tl, u, a.twW);
+      st_twiddle<P::M2, W, NSa, false>(tl, u, a.twW + P::TW.bM2);
       st_dft<P::M2, false>(u);
       __syncthreads();
       st_store<P::M2, W, NSa, 4>(line, tl, u);
@@ -374,7 +376,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
     constexpr int PS_B = (P::M1 > 1) ? 4 : PS_A;
     if constexpr (P::M1 > 1) {
       st_load<P::M1, W, PS_A>(line, tl, u);
-      st_twiddle<P::M1, W, NSb, false>(tl, u, a.twW);
+      st_twiddle<P::M1, W, NSb, false>(tl, u, a.twW + P::TW.bM1);
       st_dft<P::M1, false>(u);
       __syncthreads();
       st_store<P::M1, W, NSb, 4>(line, tl, u);
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
     }
     constexpr int NSc = NSb * P::M1;  // == W / R1
     st_load<P::R1, W, PS_B>(line, tl, u);
-    st_twiddle<P::R1, W, NSc, false>(tl, u, a.twW);
+    st_twiddle<P::R1, W, NSc, false>(tl, u, a.twW + P::TW.bR1);
     st_dft<P::R1, false>(u);
     // outputs k1 = j + r (W/R1) straight to HBM
 #pragma unroll
@@ -392,7 +394,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
       for (int r = 0; r < P::R1; ++r) {
         uint32_t k1 = j + r * (W / P::R1), c, s;
         colpair(W, k1, c, s);
-        F[faddr<R>(W, g * R + l, c, s)] = u[b * P::R1 + r];
+        st_state(F + faddr<R>(W, g * R + l, c, s), u[b * P::R1 + r], pol);
       }
     }
   }
@@ -468,16 +470,27 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   const uint32_t k1 = col ? kB : kA;
   C* cbuf = smem + col * CS;
 
+  const unsigned long long pol = l2_keep_policy();
+  // w_hN^(k1 j2) for j2 = j + (H/R1) r is base(j) * step^r: base per butterfly,
+  // step^r per column in shared memory (one rounding more than a table value)
+  OWL_SHARED_ARR(C, s_step, 32);
+  for (int i = t; i < 2 * P::R1; i += T) {
+    const int cc = i / P::R1, rr = i % P::R1;
+    s_step[cc * 16 + rr] = bigtw(a, (cc ? kB : kA) * (uint32_t)(H / P::R1) * (uint32_t)rr);
+  }
+  __syncthreads();
+
   C u[16];
   // ---- forward column DFT, first stage from HBM with the w_hN^(k1 j2) twiddle ----
 #pragma unroll
   for (int b = 0; b < 16 / P::R1; ++b) {
     int j = tc + TC * b;
+    const C base = bigtw(a, k1 * (uint32_t)j);
 #pragma unroll
     for (int r = 0; r < P::R1; ++r) {
       uint32_t j2 = j + r * (H / P::R1);
-      C x = F[faddr<R>(W, j2, c, col)];
-      u[b * P::R1 + r] = cmul(x, bigtw(a, k1 * j2));
+      C x = ld_state(F + faddr<R>(W, j2, c, col), pol);
+      u[b * P::R1 + r] = cmul(x, cmul(base, s_step[col * 16 + r]));
     }
   }
   st_dft<P::R1, false>(u);
@@ -486,7 +499,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   constexpr int PS_AFTER_M1 = (P::M1 > 1) ? 4 : PS_R1;
   if constexpr (P::M1 > 1) {
     st_load<P::M1, H, PS_R1>(cbuf, tc, u);
-    st_twiddle<P::M1, H, P::R1, false>(tc, u, a.twH);
+    st_twiddle<P::M1, H, P::R1, false>(tc, u, a.twH + P::TW.aM1);
     st_dft<P::M1, false>(u);
     __syncthreads();
     st_store<P::M1, H, P::R1, 4>(cbuf, tc, u);
@@ -495,7 +508,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   constexpr int PS_AFTER_M2 = (P::M2 > 1) ? 4 : PS_AFTER_M1;
   if constexpr (P::M2 > 1) {
     st_load<P::M2, H, PS_AFTER_M1>(cbuf, tc, u);
-    st_twiddle<P::M2, H, P::R1 * P::M1, false>(tc, u, a.twH);
+    st_twiddle<P::M2, H, P::R1 * P::M1, false>(tc, u, a.twH + P::TW.aM2);
     st_dft<P::M2, false>(u);
     __syncthreads();
     st_store<P::M2, H, P::R1 * P::M1, 4>(cbuf, tc, u);
@@ -513,8 +526,8 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   if constexpr (T > 1) {
 #pragma unroll
     for (int r = 1; r < 8; ++r) {
-      u[r] = cmul(u[r], __ldg(a.twH + r * t));
-      u[8 + r] = cmul(u[8 + r], __ldg(a.twH + r * jB));
+      u[r] = cmul(u[r], __ldg(a.twH + P::TW.aRL + r * T + t));
+      u[8 + r] = cmul(u[8 + r], __ldg(a.twH + P::TW.aRL + r * T + jB));
     }
   }
   dft8<false>(u);
@@ -531,11 +544,12 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
     return;
   } else {
     if (c != 0) {
-      const C tA = bigtw(a, kA);  // w_hN^c
+      // w_hN^(c + W k2) with k2 = t + (H/8) r is w_hN^c w_H^t w8^r
+      const C base2 = cmul(bigtw(a, kA), __ldg(a.rootH + t));
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         uint32_t k2 = t + T * r;  // A index; partner is B[H-1-k2] = u[8 + 7 - r]
-        C t2 = cmul(tA, __ldg(a.twH + k2));
+        C t2 = mul_w8<false>(base2, r);
         if constexpr (MODE == P2_SQUARE) {
           pair_sq(u[r], u[15 - r], t2);
         } else {
@@ -553,15 +567,16 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
         bufB[jB + T * r] = u[8 + r];
       }
       __syncthreads();
-      const C tB = bigtw(a, W / 2);
+      const C baseA = __ldg(a.rootH + t);
+      const C baseB = cmul(bigtw(a, W / 2), __ldg(a.rootH + jB));
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         uint32_t kA2 = t + T * r;
         uint32_t pA = (H - kA2) & (H - 1);
         uint32_t kB2 = jB + T * r;
         uint32_t pB = H - 1 - kB2;
-        C t2A = __ldg(a.twH + kA2);
-        C t2B = cmul(tB, __ldg(a.twH + kB2));
+        C t2A = mul_w8<false>(baseA, r);
+        C t2B = mul_w8<false>(baseB, r);
         if constexpr (MODE == P2_SQUARE) {
           u[r] = one_sq(u[r], bufA[pA], t2A);
           u[8 + r] = one_sq(u[8 + r], bufB[pB], t2B);
@@ -586,7 +601,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
     constexpr int PS_I1 = (P::M2 > 1) ? 4 : 3;
     if constexpr (P::M2 > 1) {
       st_load<P::M2, H, 3>(cbuf, tc, u);
-      st_twiddle<P::M2, H, 8, true>(tc, u, a.twH);
+      st_twiddle<P::M2, H, 8, true>(tc, u, a.twH + P::TW.bM2);
       st_dft<P::M2, true>(u);
       __syncthreads();
       st_store<P::M2, H, 8, 4>(cbuf, tc, u);
@@ -596,7 +611,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
     constexpr int PS_I2 = (P::M1 > 1) ? 4 : PS_I1;
     if constexpr (P::M1 > 1) {
       st_load<P::M1, H, PS_I1>(cbuf, tc, u);
-      st_twiddle<P::M1, H, NSi, true>(tc, u, a.twH);
+      st_twiddle<P::M1, H, NSi, true>(tc, u, a.twH + P::TW.bM1);
       st_dft<P::M1, true>(u);
       __syncthreads();
       st_store<P::M1, H, NSi, 4>(cbuf, tc, u);
@@ -604,15 +619,16 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
     }
     constexpr int NSl = NSi * P::M1;  // == H / R1
     st_load<P::R1, H, PS_I2>(cbuf, tc, u);
-    st_twiddle<P::R1, H, NSl, true>(tc, u, a.twH);
+    st_twiddle<P::R1, H, NSl, true>(tc, u, a.twH + P::TW.bR1);
     st_dft<P::R1, true>(u);
 #pragma unroll
     for (int b = 0; b < 16 / P::R1; ++b) {
       int j = tc + TC * b;
+      const C base = bigtw(a, k1 * (uint32_t)j);
 #pragma unroll
       for (int r = 0; r < P::R1; ++r) {
         uint32_t j2 = j + r * (H / P::R1);
-        F[faddr<R>(W, j2, c, col)] = cmulc(u[b * P::R1 + r], bigtw(a, k1 * j2));
+        st_state(F + faddr<R>(W, j2, c, col), cmulc(u[b * P::R1 + r], cmul(base, s_step[col * 16 + r])), pol);
       }
     }
   }

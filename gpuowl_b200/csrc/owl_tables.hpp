@@ -19,6 +19,8 @@
 #include <utility>
 #include <vector>
 
+#include "owl_dft.cuh"
+
 namespace owl {
 
 struct HostC {
@@ -56,12 +58,34 @@ inline uint32_t log2u(uint32_t x) {
   return r;
 }
 
+// the stage twiddle tables of a length-n line FFT in the tw_offsets(n, rl) layout
+inline std::vector<HostC> stage_tables(uint32_t n, uint32_t rl) {
+  const TwOffsets o = tw_offsets((int)n, (int)rl);
+  const uint32_t r1 = plan_r1(n, rl), m1 = plan_m1(n, rl), m2 = plan_m2(n, rl);
+  std::vector<HostC> t(o.total);
+  auto fill = [&](int off, uint32_t R, uint32_t NS) {
+    for (uint32_t r = 0; r < R; ++r) {
+      for (uint32_t k = 0; k < NS; ++k) { t[off + r * NS + k] = root((uint64_t)R * NS, (uint64_t)r * k); }
+    }
+  };
+  if (m1 > 1) { fill(o.aM1, m1, r1); }
+  if (m2 > 1) { fill(o.aM2, m2, r1 * m1); }
+  fill(o.aRL, rl, n / rl);
+  if (m2 > 1) { fill(o.bM2, m2, rl); }
+  if (m1 > 1) { fill(o.bM1, m1, rl * m2); }
+  fill(o.bR1, r1, n / r1);
+  return t;
+}
+
 struct Tables {
   uint32_t E = 0, N = 0, W = 0, H = 0, hN = 0, loShift = 0;
-  std::vector<HostC> twW, twH, twLo, twHi;
+  std::vector<HostC> twW, twH, rootH, twLo, twHi;
   std::vector<double> wt1, iwt1, wt2, iwt2;
   std::vector<uint32_t> x1, x2;
 };
+
+// lines per pass-1 block; the width FFT's cross-line radix is 16 / kLinesPerBlock
+constexpr uint32_t kLinesPerBlock = 2;
 
 inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
   if (!is_pow2(W) || !is_pow2(H)) { throw std::invalid_argument("W and H must be powers of two"); }
@@ -73,10 +97,10 @@ inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
   t.N = 2 * W * H;
   const uint32_t N = t.N;
   t.loShift = (log2u(t.hN) + 1) / 2;
-  t.twW.resize(W);
-  for (uint32_t i = 0; i < W; ++i) { t.twW[i] = root(W, i); }
-  t.twH.resize(H);
-  for (uint32_t i = 0; i < H; ++i) { t.twH[i] = root(H, i); }
+  t.twW = stage_tables(W, 16 / kLinesPerBlock);
+  t.twH = stage_tables(H, 8);
+  t.rootH.resize(H);
+  for (uint32_t i = 0; i < H; ++i) { t.rootH[i] = root(H, i); }
   uint32_t S = 1u << t.loShift;
   t.twLo.resize(S);
   for (uint32_t i = 0; i < S; ++i) { t.twLo[i] = root(t.hN, i); }

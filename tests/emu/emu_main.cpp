@@ -25,7 +25,7 @@ constexpr int kR = 2;
 struct EmuPlan {
   Tables t;
   Args a{};
-  std::vector<C> twW, twH, twLo, twHi, F1, F2;
+  std::vector<C> twW, twH, rootH, twLo, twHi, F1, F2;
   std::vector<long long> shuttle, pending;
   std::vector<uint32_t> flags;
   Ctl ctl{};
@@ -43,6 +43,7 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   p.t = make_tables(E, W, H);
   p.twW = toC(p.t.twW);
   p.twH = toC(p.t.twH);
+  p.rootH = toC(p.t.rootH);
   p.twLo = toC(p.t.twLo);
   p.twHi = toC(p.t.twHi);
   p.F1.assign(p.t.hN, make_double2(0, 0));
@@ -54,6 +55,7 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   Args& a = p.a;
   a.twW = p.twW.data();
   a.twH = p.twH.data();
+  a.rootH = p.rootH.data();
   a.twLo = p.twLo.data();
   a.twHi = p.twHi.data();
   a.wt1 = p.t.wt1.data();
