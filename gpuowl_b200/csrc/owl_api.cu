@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -330,6 +331,8 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   p->args.hN = p->hN;
   p->args.bitsLo = E / N;
   p->args.eModN = E % N;
+  p->args.scaleLo = std::ldexp(1.0, (int)(E / N));
+  p->args.iscaleLo = std::ldexp(1.0, -(int)(E / N));
   p->args.loShift = t.loShift;
   p->args.timeoutNs = 2000000000ull;
   *out = p.release();

@@ -193,17 +193,46 @@ template <int R, int N, int PS> __device__ __forceinline__ void st_load(const C*
   }
 }
 
-// tab: this stage's [r][k] table, entry r * NS + k = w_(R NS)^(r k)
+// tab: this stage's [r][k] table, entry r * NS + k = w_(R NS)^(r k). For
+// radix 8 and 16 only the rows r = 1 and r = 4 are read; the other powers come
+// from at most three products of those two correctly rounded values (each
+// within a few ulp), which keeps the L1 data path free for the exchanges.
+template <bool INV> __device__ __forceinline__ void twmul(C& v, C w) { v = cmulw<INV>(v, w); }
+
 template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twiddle(int tl, C* v, const C* __restrict__ tab) {
   if constexpr (NS > 1) {
 #pragma unroll
     for (int b = 0; b < 16 / R; ++b) {
       int j = tl + (N / 16) * b;
       int k = j & (NS - 1);
+      C* x = v + b * R;
+      if constexpr (R >= 8) {
+        const C w1 = __ldg(tab + 1 * NS + k);
+        const C w4 = __ldg(tab + 4 * NS + k);
+        const C w2 = csq(w1);
+        const C w3 = cmul(w2, w1);
+        twmul<INV>(x[1], w1);
+        twmul<INV>(x[2], w2);
+        twmul<INV>(x[3], w3);
+        twmul<INV>(x[4], w4);
+        twmul<INV>(x[5], cmul(w4, w1));
+        twmul<INV>(x[6], cmul(w4, w2));
+        twmul<INV>(x[7], cmul(w4, w3));
+        if constexpr (R == 16) {
+          const C w8 = csq(w4);
+          const C w12 = cmul(w8, w4);
+          twmul<INV>(x[8], w8);
+          twmul<INV>(x[9], cmul(w8, w1));
+          twmul<INV>(x[10], cmul(w8, w2));
+          twmul<INV>(x[11], cmul(w8, w3));
+          twmul<INV>(x[12], w12);
+          twmul<INV>(x[13], cmul(w12, w1));
+          twmul<INV>(x[14], cmul(w12, w2));
+          twmul<INV>(x[15], cmul(w12, w3));
+        }
+      } else {
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        C w = __ldg(tab + r * NS + k);
-        v[b * R + r] = cmulw<INV>(v[b * R + r], w);
+        for (int r = 1; r < R; ++r) { twmul<INV>(x[r], __ldg(tab + r * NS + k)); }
       }
     }
   }

@@ -56,6 +56,8 @@ struct Args {
   uint32_t E, N, W, H, hN;
   uint32_t bitsLo;     // E / N
   uint32_t eModN;      // E % N (a word is big iff its extra < E % N)
+  double scaleLo;      // 2^bitsLo
+  double iscaleLo;     // 2^-bitsLo
   uint32_t loShift;
   unsigned long long timeoutNs;
 };
@@ -100,6 +102,35 @@ __device__ __forceinline__ long long sext_low(long long x, uint32_t bits) {
 }
 
 constexpr double RNDVAL = 3.0 * 2251799813685248.0;  // 3 * 2^51
+
+// weight line ll of a pass-1 group: digits dgl[r][e] of column j1 = t + (W/RL) r
+// times 2^(extra/N), halved where the two table exponents wrap past N
+template <int W, int R>
+__device__ __forceinline__ void p1_weight_line(const Args& a, int t, uint32_t g, int ll, const double (&dgl)[16 / R][2],
+                                               uint32_t wrapmask, C* v) {
+  constexpr int RL = 16 / R;
+  const uint32_t j2 = g * R + ll;
+  const double w20 = __ldg(a.wt2 + 2 * j2), w21 = __ldg(a.wt2 + 2 * j2 + 1);
+#pragma unroll
+  for (int r = 0; r < RL; ++r) {
+    const uint32_t j1 = t + (W / RL) * r;
+    const double w1 = __ldg(a.wt1 + j1);
+    double y0 = dgl[r][0] * (w1 * w20);
+    double y1 = dgl[r][1] * (w1 * w21);
+    if ((wrapmask >> ((r * R + ll) * 2 + 0)) & 1u) { y0 *= 0.5; }
+    if ((wrapmask >> ((r * R + ll) * 2 + 1)) & 1u) { y1 *= 0.5; }
+    v[ll * RL + r] = mk(y0, y1);
+  }
+}
+
+// first forward width stage (radix 16/R, NS = 1) of one line, from registers to
+// shared memory
+template <int W, int R> __device__ __forceinline__ void p1_fwd_first(C* ln, int t, C* vl) {
+  constexpr int RL = 16 / R;
+  dftR<RL, false>(vl);
+#pragma unroll
+  for (int r = 0; r < RL; ++r) { ln[pad<ilog2(RL)>(t * RL + r)] = vl[r]; }
+}
 
 // ---------------------------------------------------------------------------
 // Pass 1: R lines of W points per CTA, R*W/16 threads, 16 values per thread.
@@ -194,8 +225,14 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
   }
 
   // ---- words: inverse weight, round, carry (or load digits for P1_IN) ----
+  // Fused mode keeps the digits as doubles: with power-of-two scales the split
+  // x = q 2^b + d, q = rint(x 2^-b), is exact in FP64 for |x| < 2^51, so no
+  // integer conversion is needed. The block entry/exit modes use exact integers
+  // (the exit mode must produce the canonical balanced digits).
+  double dg[R][RL][2];
   long long dig[R][RL][2];
-  uint32_t bigmask = 0;  // bit (r*R + ll)*2 + e
+  uint32_t bigmask = 0;   // bit (r*R + ll)*2 + e: word is big
+  uint32_t wrapmask = 0;  // bit (r*R + ll)*2 + e: X1 + X2 >= N (weight halved)
 #pragma unroll
   for (int r = 0; r < RL; ++r) {
     const uint32_t j1 = t + (W / RL) * r;
@@ -206,57 +243,95 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
       for (int ll = 0; ll < R; ++ll) {
         uint32_t j2 = g * R + ll;
         int2 w2 = *reinterpret_cast<const int2*>(words + 2 * ((size_t)a.H * j1 + j2));
-        dig[ll][r][0] = w2.x;
-        dig[ll][r][1] = w2.y;
+        dg[ll][r][0] = (double)w2.x;
+        dg[ll][r][1] = (double)w2.y;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          if (X1 + __ldg(a.x2 + 2 * j2 + e) >= a.N) { wrapmask |= 1u << ((r * R + ll) * 2 + e); }
+        }
       }
     } else {
       const double iw1 = __ldg(a.iwt1 + j1);
-      long long carry = ((flags & FL_LL) && g == 0 && j1 == 0) ? -2 : 0;
+      const bool ll0 = (flags & FL_LL) && g == 0 && j1 == 0;
+      double fcarry = ll0 ? -2.0 : 0.0;
+      long long carry = ll0 ? -2 : 0;
 #pragma unroll
       for (int ll = 0; ll < R; ++ll) {
         uint32_t j2 = g * R + ll;
         C z = v[ll * RL + r];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
+          const int bit = (r * R + ll) * 2 + e;
           uint32_t X2 = __ldg(a.x2 + 2 * j2 + e);
           uint32_t sum = X1 + X2;
           bool wrap = sum >= a.N;
           uint32_t extra = wrap ? sum - a.N : sum;
           bool big = extra < a.eModN;
-          if (big) { bigmask |= 1u << ((r * R + ll) * 2 + e); }
-          uint32_t bits = a.bitsLo + (big ? 1 : 0);
+          if (big) { bigmask |= 1u << bit; }
+          if (wrap) { wrapmask |= 1u << bit; }
           double iw = iw1 * __ldg(a.iwt2 + 2 * j2 + e);
           if (wrap) { iw *= 2.0; }
           double x = e ? z.y : z.x;
           double d = fma(x, iw, RNDVAL);
           double rv = d - RNDVAL;
           roe = fmaxf(roe, (float)fabs(fma(x, iw, -rv)));
-          long long n = __double_as_longlong(d) - __double_as_longlong(RNDVAL);
-          if (flags & FL_MUL3) { n *= 3; }
-          long long xx = n + carry;
-          long long dd = sext_low(xx, bits);
-          carry = (xx - dd) >> bits;
-          dig[ll][r][e] = dd;
+          if constexpr (MODE == P1_FUSED) {
+            const double sc = big ? 2.0 * a.scaleLo : a.scaleLo;
+            const double isc = big ? 0.5 * a.iscaleLo : a.iscaleLo;
+            double xx = rv + fcarry;
+            double q = fma(xx, isc, RNDVAL) - RNDVAL;
+            dg[ll][r][e] = fma(q, -sc, xx);
+            fcarry = q;
+          } else {
+            uint32_t bits = a.bitsLo + (big ? 1 : 0);
+            long long n = __double_as_longlong(d) - __double_as_longlong(RNDVAL);
+            if (flags & FL_MUL3) { n *= 3; }
+            long long xx = n + carry;
+            long long dd = sext_low(xx, bits);
+            carry = (xx - dd) >> bits;
+            dig[ll][r][e] = dd;
+          }
         }
       }
-      a.shuttle[(size_t)g * W + j1] = carry;
+      if constexpr (MODE == P1_FUSED) {
+        a.shuttle[(size_t)g * W + j1] = __double_as_longlong(fcarry);
+      } else {
+        a.shuttle[(size_t)g * W + j1] = carry;
+      }
     }
   }
 
-  if constexpr (MODE != P1_IN) {
-    // publish this group's carry row, then take the predecessor's
+  if constexpr (MODE == P1_IN) {
+#pragma unroll
+    for (int ll = 0; ll < R; ++ll) { p1_weight_line<W, R>(a, t, g, ll, dg[ll], wrapmask, v); }
+#pragma unroll
+    for (int ll = 0; ll < R; ++ll) { p1_fwd_first<W, R>(smem + ll * LS, t, v + ll * RL); }
+    __syncthreads();
+  } else {
+    // publish this group's carry row
     __threadfence();
-    // ROE: block max
     constexpr unsigned WMASK = (T >= 32) ? 0xffffffffu : ((1u << T) - 1u);
 #pragma unroll
     for (int o = (T >= 32 ? 16 : T / 2); o > 0; o >>= 1) { roe = fmaxf(roe, __shfl_xor_sync(WMASK, roe, o)); }
     if ((t & 31) == 0) { s_roe[t >> 5] = roe; }
-    __syncthreads();
+    __syncthreads();  // carries fenced; the inverse DFT's shared-memory reads are done
     if (t == 0) {
       st_release(a.flags + g, 1u);
       float m = 0.0f;
       for (int i = 0; i < (T + 31) / 32; ++i) { m = fmaxf(m, s_roe[i]); }
       if (a.roe != nullptr && roeSlot >= 0) { atomicMax(reinterpret_cast<unsigned int*>(a.roe) + roeSlot, __float_as_uint(m)); }
+    }
+    if constexpr (MODE == P1_FUSED) {
+      // lines 1..R-1 never see the carry-in in this mode: weight them and run
+      // their first forward stage while the predecessor's carries arrive
+#pragma unroll
+      for (int ll = 1; ll < R; ++ll) {
+        p1_weight_line<W, R>(a, t, g, ll, dg[ll], wrapmask, v);
+        p1_fwd_first<W, R>(smem + ll * LS, t, v + ll * RL);
+      }
+    }
+    // take the predecessor's carry row (bounded wait, decoupled lookback)
+    if (t == 0) {
       const uint32_t prev = (g == 0) ? G - 1 : g - 1;
       unsigned long long t0 = gtimer();
       bool ok = false;
@@ -272,7 +347,8 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
       }
     }
     __syncthreads();
-    // carry-in for line 0 of this group
+    // carry-in for line 0 of this group; column j1 of the last group wraps to
+    // column j1 + 1 of group 0 (and the top word's carry to word 0)
     const uint32_t prevg = (g == 0) ? G - 1 : g - 1;
 #pragma unroll
     for (int r = 0; r < RL; ++r) {
@@ -282,11 +358,13 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
       if constexpr (MODE == P1_FUSED) {
         // sloppy: two words only, the digits feed the next FFT (carryFinal,
         // src/cl/carryinc.cl:18-23)
-        uint32_t bits0 = a.bitsLo + ((bigmask >> ((r * R + 0) * 2 + 0)) & 1u);
-        long long xx = dig[0][r][0] + cin;
-        long long dd = sext_low(xx, bits0);
-        dig[0][r][0] = dd;
-        dig[0][r][1] += (xx - dd) >> bits0;
+        const bool big0 = (bigmask >> ((r * R + 0) * 2 + 0)) & 1u;
+        const double sc = big0 ? 2.0 * a.scaleLo : a.scaleLo;
+        const double isc = big0 ? 0.5 * a.iscaleLo : a.iscaleLo;
+        double xx = dg[0][r][0] + __longlong_as_double(cin);
+        double q = fma(xx, isc, RNDVAL) - RNDVAL;
+        dg[0][r][0] = fma(q, -sc, xx);
+        dg[0][r][1] += q;
       } else {
         // block exit: propagate through the thread's whole chain so that every
         // digit is balanced -- the canonical form isEqual compares (carryB,
@@ -315,52 +393,28 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
         }
       }
     }
+    if constexpr (MODE == P1_OUT) {
+      // digits to natural word order
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const uint32_t j1 = t + (W / RL) * r;
+#pragma unroll
+        for (int ll = 0; ll < R; ++ll) {
+          uint32_t j2 = g * R + ll;
+          int2 w2 = make_int2((int)dig[ll][r][0], (int)dig[ll][r][1]);
+          *reinterpret_cast<int2*>(words + 2 * ((size_t)a.H * j1 + j2)) = w2;
+        }
+      }
+      return;
+    } else {
+      p1_weight_line<W, R>(a, t, g, 0, dg[0], wrapmask, v);
+      p1_fwd_first<W, R>(smem, t, v);
+      __syncthreads();
+    }
   }
 
-  if constexpr (MODE == P1_OUT) {
-    // digits to natural word order
-#pragma unroll
-    for (int r = 0; r < RL; ++r) {
-      const uint32_t j1 = t + (W / RL) * r;
-#pragma unroll
-      for (int ll = 0; ll < R; ++ll) {
-        uint32_t j2 = g * R + ll;
-        int2 w2 = make_int2((int)dig[ll][r][0], (int)dig[ll][r][1]);
-        *reinterpret_cast<int2*>(words + 2 * ((size_t)a.H * j1 + j2)) = w2;
-      }
-    }
-    return;
-  } else {
-    // ---- weight ----
-#pragma unroll
-    for (int r = 0; r < RL; ++r) {
-      const uint32_t j1 = t + (W / RL) * r;
-      const uint32_t X1 = __ldg(a.x1 + j1);
-      const double w1 = __ldg(a.wt1 + j1);
-#pragma unroll
-      for (int ll = 0; ll < R; ++ll) {
-        uint32_t j2 = g * R + ll;
-        double y[2];
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          uint32_t X2 = __ldg(a.x2 + 2 * j2 + e);
-          double w = w1 * __ldg(a.wt2 + 2 * j2 + e);
-          if (X1 + X2 >= a.N) { w *= 0.5; }
-          y[e] = (double)dig[ll][r][e] * w;
-        }
-        v[ll * RL + r] = mk(y[0], y[1]);
-      }
-    }
-    // ---- forward width DFT: first stage across lines from registers ----
-    if constexpr (MODE != P1_IN) { __syncthreads(); }  // smem still being read by the last inverse stage
-#pragma unroll
-    for (int ll = 0; ll < R; ++ll) {
-      dftR<RL, false>(v + ll * RL);
-      C* ln = smem + ll * LS;
-#pragma unroll
-      for (int r = 0; r < RL; ++r) { ln[pad<PS_RL>(t * RL + r)] = v[ll * RL + r]; }
-    }
-    __syncthreads();
+  if constexpr (MODE != P1_OUT) {
+    // ---- rest of the forward width DFT ----
     C u[16];
     constexpr int NSa = RL;
     constexpr int PS_A = (P::M2 > 1) ? 4 : PS_RL;
@@ -469,6 +523,13 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   (void)a.E;
   const uint32_t k1 = col ? kB : kA;
   C* cbuf = smem + col * CS;
+  // the HBM-facing first (forward) and last (inverse) stages interleave the two
+  // columns across lanes, so that a warp's request covers whole 64-byte runs
+  // (both columns of R lines of one line group) of the tile layout
+  const int colI = (t >> 1) & 1;
+  const int tcI = ((t >> 2) << 1) | (t & 1);
+  const uint32_t k1I = colI ? kB : kA;
+  C* cbufI = smem + colI * CS;
 
   const unsigned long long pol = l2_keep_policy();
   // w_hN^(k1 j2) for j2 = j + (H/R1) r is base(j) * step^r: base per butterfly,
@@ -484,17 +545,17 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   // ---- forward column DFT, first stage from HBM with the w_hN^(k1 j2) twiddle ----
 #pragma unroll
   for (int b = 0; b < 16 / P::R1; ++b) {
-    int j = tc + TC * b;
-    const C base = bigtw(a, k1 * (uint32_t)j);
+    int j = tcI + TC * b;
+    const C base = bigtw(a, k1I * (uint32_t)j);
 #pragma unroll
     for (int r = 0; r < P::R1; ++r) {
       uint32_t j2 = j + r * (H / P::R1);
-      C x = ld_state(F + faddr<R>(W, j2, c, col), pol);
-      u[b * P::R1 + r] = cmul(x, cmul(base, s_step[col * 16 + r]));
+      C x = ld_state(F + faddr<R>(W, j2, c, colI), pol);
+      u[b * P::R1 + r] = cmul(x, cmul(base, s_step[colI * 16 + r]));
     }
   }
   st_dft<P::R1, false>(u);
-  st_store<P::R1, H, 1, PS_R1>(cbuf, tc, u);
+  st_store<P::R1, H, 1, PS_R1>(cbufI, tcI, u);
   __syncthreads();
   constexpr int PS_AFTER_M1 = (P::M1 > 1) ? 4 : PS_R1;
   if constexpr (P::M1 > 1) {
@@ -618,17 +679,17 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
       __syncthreads();
     }
     constexpr int NSl = NSi * P::M1;  // == H / R1
-    st_load<P::R1, H, PS_I2>(cbuf, tc, u);
-    st_twiddle<P::R1, H, NSl, true>(tc, u, a.twH + P::TW.bR1);
+    st_load<P::R1, H, PS_I2>(cbufI, tcI, u);
+    st_twiddle<P::R1, H, NSl, true>(tcI, u, a.twH + P::TW.bR1);
     st_dft<P::R1, true>(u);
 #pragma unroll
     for (int b = 0; b < 16 / P::R1; ++b) {
-      int j = tc + TC * b;
-      const C base = bigtw(a, k1 * (uint32_t)j);
+      int j = tcI + TC * b;
+      const C base = bigtw(a, k1I * (uint32_t)j);
 #pragma unroll
       for (int r = 0; r < P::R1; ++r) {
         uint32_t j2 = j + r * (H / P::R1);
-        st_state(F + faddr<R>(W, j2, c, col), cmulc(u[b * P::R1 + r], cmul(base, s_step[col * 16 + r])), pol);
+        st_state(F + faddr<R>(W, j2, c, colI), cmulc(u[b * P::R1 + r], cmul(base, s_step[colI * 16 + r])), pol);
       }
     }
   }

@@ -76,6 +76,8 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   a.hN = p.t.hN;
   a.bitsLo = E / p.t.N;
   a.eModN = E % p.t.N;
+  a.scaleLo = std::ldexp(1.0, (int)(E / p.t.N));
+  a.iscaleLo = std::ldexp(1.0, -(int)(E / p.t.N));
   a.loShift = p.t.loShift;
   a.timeoutNs = 60ull * 1000000000ull;
 }

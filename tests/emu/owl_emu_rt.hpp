@@ -82,6 +82,7 @@ template <typename T> inline T __ldg(const T* p) { return *p; }
 template <typename T> inline T __ldcg(const T* p) { return *p; }
 
 inline long long __double_as_longlong(double d) { return std::bit_cast<long long>(d); }
+inline double __longlong_as_double(long long x) { return std::bit_cast<double>(x); }
 inline unsigned __float_as_uint(float f) { return std::bit_cast<unsigned>(f); }
 
 template <typename T> inline T emu_shfl_xor(T v, int o) {
