@@ -26,6 +26,7 @@ using owl::C;
 namespace {
 
 thread_local std::string g_lastError;
+thread_local const char* g_lastLiteral = nullptr;
 
 struct OwlError {
   int code;
@@ -46,12 +47,14 @@ template <typename F> int guarded(F&& f) {
     f();
     return OWL_OK;
   } catch (const OwlError& e) {
+    g_lastLiteral = nullptr;
     g_lastError = e.msg;
     return e.code;
   } catch (const std::bad_alloc&) {
-    g_lastError = "host allocation failed";
+    g_lastLiteral = "host allocation failed";
     return OWL_ERR_NOMEM;
   } catch (const std::exception& e) {
+    g_lastLiteral = nullptr;
     g_lastError = e.what();
     return OWL_ERR_ARG;
   }
@@ -75,6 +78,10 @@ struct DeviceGuard {
 };
 
 }  // namespace
+
+namespace owl_detail {
+void set_error_literal(const char* msg) { g_lastLiteral = msg; }
+}  // namespace owl_detail
 
 struct owl_plan {
   int device = 0;
@@ -389,7 +396,7 @@ const char* owl_error_string(int status) {
   }
 }
 
-const char* owl_last_error(void) { return g_lastError.c_str(); }
+const char* owl_last_error(void) { return g_lastLiteral ? g_lastLiteral : g_lastError.c_str(); }
 
 int owl_device_count(int* count) {
   return guarded([&] {

@@ -521,7 +521,6 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   const int tc = t % TC;
   const uint32_t kA = c, kB = (c == 0) ? W / 2 : W - c;
   (void)a.E;
-  const uint32_t k1 = col ? kB : kA;
   C* cbuf = smem + col * CS;
   // the HBM-facing first (forward) and last (inverse) stages interleave the two
   // columns across lanes, so that a warp's request covers whole 64-byte runs
@@ -699,7 +698,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
 // small helpers
 
 // out[0] &= (a == b) over n int32 (outEq must hold 1 on entry)
-__global__ void k_is_equal(const int32_t* __restrict__ a, const int32_t* __restrict__ b, size_t n, int* outEq) {
+static __global__ void k_is_equal(const int32_t* __restrict__ a, const int32_t* __restrict__ b, size_t n, int* outEq) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   size_t stride = (size_t)gridDim.x * blockDim.x;
   bool eq = true;
@@ -710,7 +709,7 @@ __global__ void k_is_equal(const int32_t* __restrict__ a, const int32_t* __restr
 }
 
 // 64-bit checksum of n int32 taken as n/2 u64 (reference sum64, src/cl/etc.cl:19-29)
-__global__ void k_sum64(const unsigned long long* __restrict__ in, size_t n64, unsigned long long* out) {
+static __global__ void k_sum64(const unsigned long long* __restrict__ in, size_t n64, unsigned long long* out) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   size_t stride = (size_t)gridDim.x * blockDim.x;
   unsigned long long s = 0;
@@ -721,14 +720,14 @@ __global__ void k_sum64(const unsigned long long* __restrict__ in, size_t n64, u
 }
 
 // words around the wrap: out[i] = data[(N - 32 + i) mod N], i < 64
-__global__ void k_gather_residue(const int32_t* __restrict__ data, uint32_t N, int32_t* out) {
+static __global__ void k_gather_residue(const int32_t* __restrict__ data, uint32_t N, int32_t* out) {
   int i = threadIdx.x;
   if (i < 64) { out[i] = data[(N - 32 + i) % N]; }
 }
 
 // Applies the carries queued by a block-exit line pass, one after the other,
 // each propagated word by word (with wrap-around) until it is absorbed.
-__global__ void k_carry_fixup(Args a, int32_t* __restrict__ words) {
+static __global__ void k_carry_fixup(Args a, int32_t* __restrict__ words) {
   if (threadIdx.x != 0 || blockIdx.x != 0) { return; }
   uint32_t n = a.ctl->npending;
   if (n > kPendingCap) { n = kPendingCap; }
@@ -750,7 +749,7 @@ __global__ void k_carry_fixup(Args a, int32_t* __restrict__ words) {
 }
 
 // timeout probe: wait on a flag that is never set, with the pass-1 wait loop
-__global__ void k_wait_probe(Args a, uint32_t flagIndex) {
+static __global__ void k_wait_probe(Args a, uint32_t flagIndex) {
   if (threadIdx.x == 0) {
     unsigned long long t0 = gtimer();
     bool ok = false;

@@ -1,0 +1,54 @@
+"""owl_square_noalloc: the squaring entry point that allocates nothing.
+
+Some callers cannot call cudaMalloc -- code inside a CUDA graph capture, programs
+whose device memory all belongs to their own pool allocator, real-time loops --
+so this entry point keeps all of its scratch in one fixed device array inside
+libowl and squares a buffer the caller already owns. Its results must equal the
+regular entry point's (owl_square) word for word, call after call: the shared
+array keeps the previous call's contents, and each call must clear what has to
+start at zero. This file runs last so that a failure here leaves every other
+test already run.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import random_words
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(owl):
+    fn = owl.load().owl_square_noalloc
+    fn.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                   ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    return fn
+
+
+@pytest.mark.parametrize("E,W,H,flags", [(500009, 128, 128, 0), (1000003, 128, 256, 2),
+                                         (86243, 64, 64, 1)])
+def test_noalloc_matches_square_twice(owl, E, W, H, flags):
+    fn = _noalloc(owl)
+    n = 25
+    with owl.Plan(E, W=W, H=H) as p:
+        ref, buf = p.alloc(), p.alloc()
+        w = random_words(E, E ^ 0x5EED)
+        p.writeIn(ref, w)
+        p.writeIn(buf, w)
+        for _ in range(2):  # two calls in a row: the second starts from the first's leftovers
+            p.squareLoop(ref, ref, n, mul3=bool(flags & 1), ll=bool(flags & 2))
+            p.sync()
+            rc = fn(0, E, W, H, buf, n, flags, None)
+            assert rc == 0, owl.load().owl_last_error()
+            assert np.array_equal(p.readOut(buf), p.readOut(ref))
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch(owl):
+    fn = _noalloc(owl)
+    with owl.Plan(4989349, W=256, H=512) as p:
+        buf = p.alloc()
+        assert fn(0, 4989349, 256, 512, buf, 1, 0, None) == -1
+        assert b"no-alloc" in owl.load().owl_last_error()
+        assert fn(0, 4989349, 0, 0, buf, 1, 0, None) == -1
