@@ -319,6 +319,8 @@ def run_ours(args, rank, world, local):
                                "plain FP64 form",
                    "E": E_8M, "N": N_8M, "block": B, "step": "modMul(check,data) + %d squarings" % B,
                    "timed_iterations": args.steps * B, "l2": "flushed (512 MiB write) between timed steps",
+                   "timing": "step: CUDA events on the plan's stream around modMul + a graph-launched block; "
+                             "kernels: per-launch %globaltimer stamps (first CTA start, last CTA end) in the same steps",
                    "parallelism": "replicas x%d" % world},
         "res64_match_golden": res_match, "res64_checked": n, "gerbicz_ok": bool(gerbicz_ok),
         "max_roe": round(float(roe.max()), 5) if roe.size else None,

@@ -97,6 +97,17 @@ struct owl_plan {
   int* eq = nullptr;
   uint32_t roePos = 0;
   std::vector<int32_t*> bufs;
+  // squaring blocks captured as CUDA graphs, keyed by (in, out, n, flags, with events)
+  struct GraphEntry {
+    const int32_t* in;
+    int32_t* out;
+    uint32_t n, flags;
+    bool profiled;
+    cudaGraphExec_t exec;
+    uint64_t lastUse;
+  };
+  std::vector<GraphEntry> graphs;
+  uint64_t useClock = 0;
 };
 
 namespace {
@@ -114,36 +125,36 @@ template <int H, int M> void setp2attr() {
      "cudaFuncSetAttribute(pass2)");
 }
 
-template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags) {
+template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags, int ts) {
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
   dim3 grid(p->H / kR);
   switch (mode) {
     case owl::P1_FUSED:
-      owl::k_pass1<W, kR, owl::P1_FUSED><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags);
+      owl::k_pass1<W, kR, owl::P1_FUSED><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
       break;
     case owl::P1_IN:
-      owl::k_pass1<W, kR, owl::P1_IN><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags);
+      owl::k_pass1<W, kR, owl::P1_IN><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
       break;
     default:
-      owl::k_pass1<W, kR, owl::P1_OUT><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags);
+      owl::k_pass1<W, kR, owl::P1_OUT><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
       break;
   }
 }
 
-template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq) {
+template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts) {
   constexpr int T = H / 8;
   size_t sm = 2 * (size_t)owl::p2_col_stride<H>() * sizeof(C);
   dim3 grid(p->W / 2);
   switch (mode) {
     case owl::P2_SQUARE:
-      owl::k_pass2<H, kR, owl::P2_SQUARE><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq);
+      owl::k_pass2<H, kR, owl::P2_SQUARE><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
       break;
     case owl::P2_FWD:
-      owl::k_pass2<H, kR, owl::P2_FWD><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq);
+      owl::k_pass2<H, kR, owl::P2_FWD><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
       break;
     default:
-      owl::k_pass2<H, kR, owl::P2_MUL><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq);
+      owl::k_pass2<H, kR, owl::P2_MUL><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
       break;
   }
 }
@@ -177,16 +188,21 @@ void set_attrs(uint32_t W, uint32_t H) {
   }
 }
 
-void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags) {
+void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot = -1, int ts = -1) {
   int slot = -1;
   if (mode != owl::P1_IN) {
-    slot = (int)std::min(p->roePos, kRoeCap - 1);
-    if (p->roePos < kRoeCap) { ++p->roePos; }
+    if (fixedSlot >= 0) {
+      slot = std::min(fixedSlot, (int)kRoeCap - 1);
+      p->roePos = std::max(p->roePos, (uint32_t)slot + 1);
+    } else {
+      slot = (int)std::min(p->roePos, kRoeCap - 1);
+      if (p->roePos < kRoeCap) { ++p->roePos; }
+    }
   }
   switch (p->W) {
 #define CASE_W(n)                                \
   case n:                                        \
-    p1launch<n>(p, mode, F, words, slot, flags); \
+    p1launch<n>(p, mode, F, words, slot, flags, ts); \
     break;
     OWL_FOR_SIZES(CASE_W)
 #undef CASE_W
@@ -196,11 +212,11 @@ void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags) {
   ck(cudaGetLastError(), "pass1 launch");
 }
 
-void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq) {
+void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts = -1) {
   switch (p->H) {
 #define CASE_H(n)                       \
   case n:                               \
-    p2launch<n>(p, mode, F, Fb, Fq);    \
+    p2launch<n>(p, mode, F, Fb, Fq, ts); \
     break;
     OWL_FOR_SIZES(CASE_H)
 #undef CASE_H
@@ -211,10 +227,85 @@ void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq) {
 }
 
 // the block-exit line pass, then the (normally empty) queue of leftover carries
-void pass1_out(owl_plan* p, int32_t* words, int flags) {
-  pass1(p, owl::P1_OUT, p->F1, words, flags);
+void pass1_out(owl_plan* p, int32_t* words, int flags, int fixedSlot = -1, int ts = -1) {
+  pass1(p, owl::P1_OUT, p->F1, words, flags, fixedSlot, ts);
   owl::k_carry_fixup<<<1, 32, 0, p->stream>>>(p->args, words);
   ck(cudaGetLastError(), "fixup launch");
+}
+
+constexpr uint32_t kTsCap = 4096;  // launch-timestamp slots (profiled blocks of up to 2047 squarings)
+
+// Enqueues n squarings in -> out on the plan's stream: entry line pass, n x
+// (column pass, line pass), exit fixup. ROE slot k holds squaring k's
+// round-off. With `stamp`, launch i records its first CTA start and last CTA
+// end in timestamp slot i (launch 0 is the entry pass, 2k+1 / 2k+2 are
+// squaring k's column and line passes).
+void enqueue_square(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags, bool stamp) {
+  const int ll = (flags & OWL_SQ_LL) ? owl::FL_LL : 0;
+  const int mul3 = (flags & OWL_SQ_MUL3) ? owl::FL_MUL3 : 0;
+  int li = 0;
+  auto ts = [&] { return stamp ? li++ : -1; };
+  if (stamp) {
+    const size_t cnt = 2 * (size_t)n + 1;
+    ck(cudaMemsetAsync(p->args.tsStart, 0xff, cnt * sizeof(unsigned long long), p->stream), "memset ts");
+    ck(cudaMemsetAsync(p->args.tsEnd, 0, cnt * sizeof(unsigned long long), p->stream), "memset ts");
+  }
+  pass1(p, owl::P1_IN, p->F1, const_cast<int32_t*>(in), 0, -1, ts());
+  for (uint32_t k = 0; k < n; ++k) {
+    pass2(p, owl::P2_SQUARE, p->F1, nullptr, nullptr, ts());
+    if (k + 1 < n) {
+      pass1(p, owl::P1_FUSED, p->F1, nullptr, ll, (int)k, ts());
+    } else {
+      pass1_out(p, out, ll | mul3, (int)k, ts());
+    }
+  }
+}
+
+constexpr uint32_t kGraphMinIters = 16;
+constexpr size_t kGraphCacheMax = 8;
+
+// the cached graph for this block, captured on first use
+owl_plan::GraphEntry& graph_for(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags,
+                                bool profiled) {
+  ++p->useClock;
+  for (auto& g : p->graphs) {
+    if (g.in == in && g.out == out && g.n == n && g.flags == flags && g.profiled == profiled) {
+      g.lastUse = p->useClock;
+      return g;
+    }
+  }
+  if (p->graphs.size() >= kGraphCacheMax) {
+    auto lru = std::min_element(p->graphs.begin(), p->graphs.end(),
+                                [](const auto& a, const auto& b) { return a.lastUse < b.lastUse; });
+    cudaGraphExecDestroy(lru->exec);
+    p->graphs.erase(lru);
+  }
+  owl_plan::GraphEntry g{in, out, n, flags, profiled, nullptr, p->useClock};
+  cudaGraph_t graph = nullptr;
+  ck(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  try {
+    enqueue_square(p, out, in, n, flags, profiled);
+  } catch (...) {
+    cudaStreamEndCapture(p->stream, &graph);
+    if (graph) { cudaGraphDestroy(graph); }
+    throw;
+  }
+  ck(cudaStreamEndCapture(p->stream, &graph), "cudaStreamEndCapture");
+  cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  ck(e, "cudaGraphInstantiate");
+  p->graphs.push_back(std::move(g));
+  return p->graphs.back();
+}
+
+void run_square(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags) {
+  if (n < kGraphMinIters) {
+    enqueue_square(p, out, in, n, flags, false);
+    return;
+  }
+  auto& g = graph_for(p, out, in, n, flags, false);
+  ck(cudaGraphLaunch(g.exec, p->stream), "cudaGraphLaunch");
+  p->roePos = std::max(p->roePos, std::min(n, kRoeCap));
 }
 
 void check_plan(const owl_plan* p) {
@@ -316,8 +407,8 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
 
   // scratch: carry shuttle, flags, control word, ROE slots, small outputs
   const uint32_t G = H / kR;
-  size_t sbytes = 256 * 9 + (size_t)G * W * sizeof(long long) + G * sizeof(uint32_t) + sizeof(owl::Ctl) +
-                  2 * owl::kPendingCap * sizeof(long long) +
+  size_t sbytes = 256 * 11 + (size_t)G * W * sizeof(long long) + G * sizeof(uint32_t) + sizeof(owl::Ctl) +
+                  2 * owl::kPendingCap * sizeof(long long) + 2 * kTsCap * sizeof(unsigned long long) +
                   kRoeCap * sizeof(float) + 64 * sizeof(int32_t) + sizeof(unsigned long long) + sizeof(int);
   ck(cudaMalloc(&p->scratch, sbytes), "cudaMalloc(scratch)");
   ck(cudaMemset(p->scratch, 0, sbytes), "memset(scratch)");
@@ -326,6 +417,8 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   p->args.flags = carve<uint32_t>(cur, G);
   p->args.ctl = carve<owl::Ctl>(cur, 1);
   p->args.pending = carve<long long>(cur, 2 * owl::kPendingCap);
+  p->args.tsStart = carve<unsigned long long>(cur, kTsCap);
+  p->args.tsEnd = carve<unsigned long long>(cur, kTsCap);
   p->args.roe = carve<float>(cur, kRoeCap);
   p->small = carve<int32_t>(cur, 64);
   p->sum = carve<unsigned long long>(cur, 1);
@@ -348,6 +441,7 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
 void plan_destroy(owl_plan* p) {
   DeviceGuard dg(p->device);
   if (p->stream) { cudaStreamSynchronize(p->stream); }
+  for (auto& g : p->graphs) { cudaGraphExecDestroy(g.exec); }
   for (int32_t* b : p->bufs) { cudaFree(b); }
   cudaFree(p->F1);
   cudaFree(p->F2);
@@ -578,17 +672,7 @@ int owl_square(owl_plan* plan, int32_t* out, const int32_t* in, uint32_t n, uint
       return;
     }
     DeviceGuard dg(plan->device);
-    const int ll = (flags & OWL_SQ_LL) ? owl::FL_LL : 0;
-    const int mul3 = (flags & OWL_SQ_MUL3) ? owl::FL_MUL3 : 0;
-    pass1(plan, owl::P1_IN, plan->F1, const_cast<int32_t*>(in), 0);
-    for (uint32_t k = 0; k < n; ++k) {
-      pass2(plan, owl::P2_SQUARE, plan->F1, nullptr, nullptr);
-      if (k + 1 < n) {
-        pass1(plan, owl::P1_FUSED, plan->F1, nullptr, ll);
-      } else {
-        pass1_out(plan, out, ll | mul3);
-      }
-    }
+    run_square(plan, out, in, n, flags & (OWL_SQ_LL | OWL_SQ_MUL3));
   });
 }
 
@@ -705,43 +789,29 @@ int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint
   return guarded([&] {
     check_plan(plan);
     check_buf(plan, buf);
-    if (!ms || !launches || n == 0) { fail(OWL_ERR_ARG, "bad argument"); }
+    if (!ms || !launches || n == 0 || 2 * n + 1 > kTsCap) { fail(OWL_ERR_ARG, "bad argument"); }
     DeviceGuard dg(plan->device);
-    std::vector<cudaEvent_t> ev(2 * n + 2);
-    for (auto& e : ev) { ck(cudaEventCreate(&e), "cudaEventCreate"); }
-    struct Rel {
-      std::vector<cudaEvent_t>& v;
-      ~Rel() { for (auto e : v) { cudaEventDestroy(e); } }
-    } rel{ev};
-    ck(cudaEventRecord(ev[0], plan->stream), "record");
-    pass1(plan, owl::P1_IN, plan->F1, buf, 0);
-    ck(cudaEventRecord(ev[1], plan->stream), "record");
-    for (uint32_t k = 0; k < n; ++k) {
-      pass2(plan, owl::P2_SQUARE, plan->F1, nullptr, nullptr);
-      ck(cudaEventRecord(ev[2 + 2 * k], plan->stream), "record");
-      if (k + 1 < n) {
-        pass1(plan, owl::P1_FUSED, plan->F1, nullptr, 0);
-      } else {
-        pass1_out(plan, buf, 0);
-      }
-      ck(cudaEventRecord(ev[3 + 2 * k], plan->stream), "record");
-    }
+    auto& g = graph_for(plan, buf, buf, n, 0, true);
+    ck(cudaGraphLaunch(g.exec, plan->stream), "cudaGraphLaunch");
+    plan->roePos = std::max(plan->roePos, std::min(n, kRoeCap));
+    const size_t cnt = 2 * (size_t)n + 1;
+    std::vector<unsigned long long> t0(cnt), t1(cnt);
+    ck(cudaMemcpyAsync(t0.data(), plan->args.tsStart, cnt * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       plan->stream), "read ts");
+    ck(cudaMemcpyAsync(t1.data(), plan->args.tsEnd, cnt * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       plan->stream), "read ts");
     sync_and_check(plan);
-    float t2 = 0, t1 = 0, te = 0, x = 0;
-    ck(cudaEventElapsedTime(&x, ev[0], ev[1]), "elapsed");
-    te += x;
-    for (uint32_t k = 0; k < n; ++k) {
-      ck(cudaEventElapsedTime(&x, ev[1 + 2 * k], ev[2 + 2 * k]), "elapsed");
-      t2 += x;
-      ck(cudaEventElapsedTime(&x, ev[2 + 2 * k], ev[3 + 2 * k]), "elapsed");
-      if (k + 1 < n) { t1 += x; } else { te += x; }
+    double t2ms = 0, t1ms = 0, tems = 0;
+    for (size_t i = 0; i < cnt; ++i) {
+      double d = (t1[i] > t0[i]) ? (double)(t1[i] - t0[i]) * 1e-6 : 0.0;
+      if (i == 0 || i + 1 == cnt) { tems += d; } else if (i % 2 == 1) { t2ms += d; } else { t1ms += d; }
     }
-    ms[0] = t2;
-    ms[1] = t1;
-    ms[2] = te;
+    ms[0] = (float)t2ms;
+    ms[1] = (float)t1ms;
+    ms[2] = (float)tems;
     launches[0] = n;
     launches[1] = n - 1;
-    launches[2] = 3;
+    launches[2] = 2;
   });
 }
 

@@ -53,6 +53,8 @@ struct Args {
   uint32_t* flags;     // per line group
   Ctl* ctl;
   float* roe;          // per-launch max round-off slots
+  unsigned long long* tsStart;  // per-launch earliest CTA start (%globaltimer), profiling only
+  unsigned long long* tsEnd;    // per-launch latest CTA end
   uint32_t E, N, W, H, hN;
   uint32_t bitsLo;     // E / N
   uint32_t eModN;      // E % N (a word is big iff its extra < E % N)
@@ -103,6 +105,14 @@ __device__ __forceinline__ long long sext_low(long long x, uint32_t bits) {
 
 constexpr double RNDVAL = 3.0 * 2251799813685248.0;  // 3 * 2^51
 
+// launch timestamps for the profiler: slot < 0 turns them off
+__device__ __forceinline__ void ts_begin(const Args& a, int slot) {
+  if (slot >= 0 && threadIdx.x == 0) { atomicMin(a.tsStart + slot, gtimer()); }
+}
+__device__ __forceinline__ void ts_end(const Args& a, int slot) {
+  if (slot >= 0 && threadIdx.x == 0) { atomicMax(a.tsEnd + slot, gtimer()); }
+}
+
 // weight line ll of a pass-1 group: digits dgl[r][e] of column j1 = t + (W/RL) r
 // times 2^(extra/N), halved where the two table exponents wrap past N
 template <int W, int R>
@@ -136,7 +146,7 @@ template <int W, int R> __device__ __forceinline__ void p1_fwd_first(C* ln, int 
 // Pass 1: R lines of W points per CTA, R*W/16 threads, 16 values per thread.
 template <int W, int R, int MODE>
 __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
-    k_pass1(Args a, C* __restrict__ F, int32_t* __restrict__ words, int roeSlot, int flags) {
+    k_pass1(Args a, C* __restrict__ F, int32_t* __restrict__ words, int roeSlot, int flags, int tslot) {
   constexpr int T = R * W / 16;
   constexpr int RL = 16 / R;
   using P = Plan<W, RL>;
@@ -147,6 +157,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
   OWL_SHARED(uint32_t, s_g);
   OWL_SHARED_ARR(float, s_roe, 32);
 
+  ts_begin(a, tslot);
   const int t = threadIdx.x;
   const uint32_t G = a.H / R;
   uint32_t g;
@@ -405,6 +416,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
           *reinterpret_cast<int2*>(words + 2 * ((size_t)a.H * j1 + j2)) = w2;
         }
       }
+      ts_end(a, tslot);
       return;
     } else {
       p1_weight_line<W, R>(a, t, g, 0, dg[0], wrapmask, v);
@@ -451,6 +463,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
         st_state(F + faddr<R>(W, g * R + l, c, s), u[b * P::R1 + r], pol);
       }
     }
+    ts_end(a, tslot);
   }
 }
 
@@ -506,7 +519,7 @@ __device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
 
 template <int H, int R, int MODE>
 __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
-    k_pass2(Args a, C* __restrict__ F, const C* __restrict__ Fb, C* __restrict__ Fq) {
+    k_pass2(Args a, C* __restrict__ F, const C* __restrict__ Fb, C* __restrict__ Fq, int tslot) {
   constexpr int T = H / 8;
   constexpr int TC = H / 16;  // threads per column in the per-column stages
   using P = Plan<H, 8>;
@@ -516,6 +529,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
 
   const uint32_t W = a.W;
   const uint32_t c = blockIdx.x;
+  ts_begin(a, tslot);
   const int t = threadIdx.x;
   const int col = t / TC;
   const int tc = t % TC;
@@ -601,6 +615,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
       Fq[faddr<R>(W, kA2, c, 0)] = u[r];
       Fq[faddr<R>(W, kB2, c, 1)] = u[8 + r];
     }
+    ts_end(a, tslot);
     return;
   } else {
     if (c != 0) {
@@ -691,6 +706,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
         st_state(F + faddr<R>(W, j2, c, colI), cmulc(u[b * P::R1 + r], cmul(base, s_step[colI * 16 + r])), pol);
       }
     }
+    ts_end(a, tslot);
   }
 }
 

@@ -147,16 +147,16 @@ template <int W> void p1(const owl::Args& a, int mode, owl::C* F, int32_t* words
   const dim3 grid(a.H / kR);
   const int slot = (int)(kRoeSlots - 1);
   if (mode == owl::P1_IN) {
-    owl::k_pass1<W, kR, owl::P1_IN><<<grid, T, sm, s>>>(a, F, words, slot, flags);
+    owl::k_pass1<W, kR, owl::P1_IN><<<grid, T, sm, s>>>(a, F, words, slot, flags, -1);
   } else if (mode == owl::P1_FUSED) {
-    owl::k_pass1<W, kR, owl::P1_FUSED><<<grid, T, sm, s>>>(a, F, words, slot, flags);
+    owl::k_pass1<W, kR, owl::P1_FUSED><<<grid, T, sm, s>>>(a, F, words, slot, flags, -1);
   } else {
-    owl::k_pass1<W, kR, owl::P1_OUT><<<grid, T, sm, s>>>(a, F, words, slot, flags);
+    owl::k_pass1<W, kR, owl::P1_OUT><<<grid, T, sm, s>>>(a, F, words, slot, flags, -1);
   }
 }
 template <int H> void p2(const owl::Args& a, owl::C* F, cudaStream_t s) {
   const size_t sm = 2 * (size_t)owl::p2_col_stride<H>() * sizeof(owl::C);
-  owl::k_pass2<H, kR, owl::P2_SQUARE><<<a.W / 2, H / 8, sm, s>>>(a, F, nullptr, nullptr);
+  owl::k_pass2<H, kR, owl::P2_SQUARE><<<a.W / 2, H / 8, sm, s>>>(a, F, nullptr, nullptr, -1);
 }
 
 void launch_p1(const owl::Args& a, int mode, owl::C* F, int32_t* words, int flags, cudaStream_t s) {

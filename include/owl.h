@@ -112,10 +112,11 @@ int owl_sync(owl_plan* plan);
    record CUDA events on the stream the engine's kernels run on. */
 int owl_plan_stream(owl_plan* plan, void** stream);
 
-/* Per-kernel timing of n squarings of buf (in place), the counterpart of the reference's
-   -time profile (src/Gpu.cpp:773-799, src/Queue.cpp:54-58): CUDA events bracket every launch.
-   ms[0] = total pass-2 (column) time, ms[1] = total pass-1 (line/carry) time, ms[2] = total
-   of the block's entry/exit launches; launches[0..2] the matching launch counts. */
+/* n squarings of buf (in place, n <= 2047) with per-kernel device time, the counterpart of the
+   reference's -time profile (src/Gpu.cpp:773-799, src/Queue.cpp:54-58). The block runs as the
+   same CUDA graph as owl_square; each kernel launch stamps its first CTA start and last CTA end
+   with the GPU's global timer. ms[0] = total pass-2 (column) time, ms[1] = total pass-1
+   (line/carry) time, ms[2] = entry and exit passes; launches[0..2] the matching counts. */
 int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint32_t* launches);
 
 /* Failure-detection probe: one device wait on a flag nothing sets, with the plan's

@@ -86,13 +86,13 @@ template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * p1_line_stride<W, kR>() * sizeof(C);
   Args a = p.a;
-  emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M>(a, F, words, slot, flags); });
+  emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M>(a, F, words, slot, flags, -1); });
 }
 template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {
   constexpr int T = H / 8;
   size_t sm = 2 * (size_t)p2_col_stride<H>() * sizeof(C);
   Args a = p.a;
-  emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M>(a, F, Fb, Fq); });
+  emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M>(a, F, Fb, Fq, -1); });
 }
 
 template <int W> void p1w(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {

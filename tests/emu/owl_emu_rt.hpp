@@ -122,6 +122,20 @@ inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v)
 inline unsigned atomicExch(unsigned* p, unsigned v) { return std::atomic_ref<unsigned>(*p).exchange(v); }
 inline unsigned atomicOr(unsigned* p, unsigned v) { return std::atomic_ref<unsigned>(*p).fetch_or(v); }
 inline int atomicAnd(int* p, int v) { return std::atomic_ref<int>(*p).fetch_and(v); }
+inline unsigned long long atomicMin(unsigned long long* p, unsigned long long v) {
+  std::atomic_ref<unsigned long long> a(*p);
+  unsigned long long cur = a.load();
+  while (cur > v && !a.compare_exchange_weak(cur, v)) {
+  }
+  return cur;
+}
+inline unsigned long long atomicMax(unsigned long long* p, unsigned long long v) {
+  std::atomic_ref<unsigned long long> a(*p);
+  unsigned long long cur = a.load();
+  while (cur < v && !a.compare_exchange_weak(cur, v)) {
+  }
+  return cur;
+}
 inline unsigned atomicMax(unsigned* p, unsigned v) {
   std::atomic_ref<unsigned> a(*p);
   unsigned cur = a.load();
