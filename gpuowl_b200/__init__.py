@@ -13,7 +13,8 @@ import os
 
 import numpy as np
 
-__all__ = ["OwlError", "load", "Plan", "n_words", "fft_choose", "LIB_PATH"]
+__all__ = ["OwlError", "load", "Plan", "n_words", "fft_choose", "LIB_PATH", "prp_run", "ll_run",
+           "prp_save", "prp_load", "ll_save", "ll_load", "crc32"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libowl.so")
@@ -37,6 +38,21 @@ _P = ctypes.c_void_p
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _U32P = ctypes.POINTER(ctypes.c_uint32)
 _U64P = ctypes.POINTER(ctypes.c_uint64)
+
+class RunOpts(ctypes.Structure):
+    """owl_run_opts (include/owl_host.h)."""
+    _fields_ = [("block_size", ctypes.c_uint32), ("log_step", ctypes.c_uint32), ("check_step", ctypes.c_uint32),
+                ("stop_after", ctypes.c_uint32), ("n_savefiles", ctypes.c_uint32), ("W", ctypes.c_uint32),
+                ("H", ctypes.c_uint32), ("save_dir", ctypes.c_char_p), ("inject_fault_k", ctypes.c_uint32),
+                ("verbose", ctypes.c_int), ("res_cap", ctypes.c_uint32), ("res_k", ctypes.POINTER(ctypes.c_uint32)),
+                ("res_res64", ctypes.POINTER(ctypes.c_uint64)), ("res_n", ctypes.POINTER(ctypes.c_uint32))]
+
+
+class RunResult(ctypes.Structure):
+    """owl_run_result (include/owl_host.h)."""
+    _fields_ = [("is_prime", ctypes.c_int), ("finished", ctypes.c_int), ("k", ctypes.c_uint32),
+                ("res64", ctypes.c_uint64), ("n_errors", ctypes.c_uint32), ("res2048", ctypes.c_char * 513)]
+
 
 _SIGS = {
     "owl_abi_version": ([], ctypes.c_int),
@@ -68,6 +84,15 @@ _SIGS = {
     "owl_sync": ([_P], ctypes.c_int),
     "owl_probe_wait_timeout": ([_P], ctypes.c_int),
     "owl_plan_stream": ([_P, ctypes.POINTER(_P)], ctypes.c_int),
+    "owl_prp_run": ([ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(RunOpts), ctypes.POINTER(RunResult)], ctypes.c_int),
+    "owl_ll_run": ([ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(RunOpts), ctypes.POINTER(RunResult)], ctypes.c_int),
+    "owl_prp_save": ([ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _U32P,
+                      ctypes.c_uint32, ctypes.c_double], ctypes.c_int),
+    "owl_prp_load": ([ctypes.c_char_p, ctypes.c_uint32, _U32P, _U32P, _U64P, _U32P, _U32P,
+                      ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "owl_ll_save": ([ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, _U32P, ctypes.c_double], ctypes.c_int),
+    "owl_ll_load": ([ctypes.c_char_p, ctypes.c_uint32, _U32P, _U32P, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "owl_crc32": ([ctypes.c_void_p, ctypes.c_size_t], ctypes.c_uint32),
     "owl_profile_square": ([_P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), _U32P], ctypes.c_int),
 }
 
@@ -241,3 +266,64 @@ class Plan:
     def probe_wait_timeout(self):
         """Returns the status of a device wait that must time out (ERR_TIMEOUT)."""
         return self.lib.owl_probe_wait_timeout(self.h)
+
+
+# ---- host drivers (include/owl_host.h) ----
+
+def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, W, H, inject_fault_k, verbose,
+         n_savefiles=4, cap=4096):
+    lib = load()
+    ks = (ctypes.c_uint32 * cap)()
+    rs = (ctypes.c_uint64 * cap)()
+    n = ctypes.c_uint32(0)
+    o = RunOpts(block, log_step, check_step, stop_after, n_savefiles, W, H,
+                save_dir.encode() if save_dir else None, inject_fault_k, 1 if verbose else 0, cap,
+                ks, rs, ctypes.pointer(n))
+    r = RunResult()
+    _check(getattr(lib, fn_name)(device, E, ctypes.byref(o), ctypes.byref(r)))
+    return {"is_prime": bool(r.is_prime), "finished": bool(r.finished), "k": r.k, "res64": r.res64,
+            "n_errors": r.n_errors, "res2048": r.res2048.decode(),
+            "checkpoints": [(ks[i], rs[i]) for i in range(n.value)]}
+
+
+def prp_run(E, device=0, block=1000, log_step=20000, check_step=0, stop_after=0, save_dir=None, W=0, H=0,
+            inject_fault_k=0, verbose=False):
+    """PRP-3 test (the reference's Gpu::isPrimePRP) through owl_prp_run."""
+    return _run("owl_prp_run", E, device, block, log_step, check_step, stop_after, save_dir, W, H,
+                inject_fault_k, verbose)
+
+
+def ll_run(E, device=0, log_step=10000, stop_after=0, save_dir=None, W=0, H=0, verbose=False):
+    """Lucas-Lehmer test (the reference's Gpu::isPrimeLL) through owl_ll_run."""
+    return _run("owl_ll_run", E, device, 1000, log_step, 0, stop_after, save_dir, W, H, 0, verbose)
+
+
+def prp_save(save_dir, E, k, block, res64, check, n_errors=0, elapsed=0.0):
+    c = np.ascontiguousarray(check, dtype=np.uint32)
+    _check(load().owl_prp_save(save_dir.encode(), E, k, block, res64, c.ctypes.data_as(_U32P), n_errors, elapsed))
+
+
+def prp_load(save_dir, E):
+    k, b, ne = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    r, el = ctypes.c_uint64(), ctypes.c_double()
+    c = np.zeros(n_words(E), dtype=np.uint32)
+    _check(load().owl_prp_load(save_dir.encode(), E, ctypes.byref(k), ctypes.byref(b), ctypes.byref(r),
+                               c.ctypes.data_as(_U32P), ctypes.byref(ne), ctypes.byref(el)))
+    return {"k": k.value, "block": b.value, "res64": r.value, "check": c, "n_errors": ne.value, "elapsed": el.value}
+
+
+def ll_save(save_dir, E, k, data, elapsed=0.0):
+    d = np.ascontiguousarray(data, dtype=np.uint32)
+    _check(load().owl_ll_save(save_dir.encode(), E, k, d.ctypes.data_as(_U32P), elapsed))
+
+
+def ll_load(save_dir, E):
+    k, el = ctypes.c_uint32(), ctypes.c_double()
+    d = np.zeros(n_words(E), dtype=np.uint32)
+    _check(load().owl_ll_load(save_dir.encode(), E, ctypes.byref(k), d.ctypes.data_as(_U32P), ctypes.byref(el)))
+    return {"k": k.value, "data": d, "elapsed": el.value}
+
+
+def crc32(data):
+    b = bytes(data)
+    return load().owl_crc32(b, len(b))

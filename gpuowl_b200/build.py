@@ -1,9 +1,10 @@
-"""Build libowl.so (the sm_100a engine behind include/owl.h) in-tree.
+"""Build libowl.so (the sm_100a engine behind include/owl.h and the host drivers of
+include/owl_host.h) in-tree.
 
     python -m gpuowl_b200.build            # or: python gpuowl_b200/build.py
 
-Compiles gpuowl_b200/csrc/*.cu with nvcc for sm_100a only and links
-gpuowl_b200/libowl.so. The build is skipped when the library is newer than
+Compiles gpuowl_b200/csrc/*.cu with nvcc for sm_100a only, gpuowl_b200/host/*.cpp
+with the host compiler nvcc drives, and links gpuowl_b200/libowl.so. The build is skipped when the library is newer than
 every source file.
 """
 import os
@@ -13,6 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
+HOST = os.path.join(HERE, "host")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libowl.so")
 
@@ -30,10 +32,12 @@ def nvcc():
 
 def sources():
     out = []
-    for name in sorted(os.listdir(CSRC)):
-        if name.endswith((".cu", ".cuh", ".hpp", ".h", ".cpp")):
-            out.append(os.path.join(CSRC, name))
-    out.append(os.path.join(INCLUDE, "owl.h"))
+    for d in (CSRC, HOST):
+        for name in sorted(os.listdir(d)):
+            if name.endswith((".cu", ".cuh", ".hpp", ".h", ".cpp")):
+                out.append(os.path.join(d, name))
+    for name in sorted(os.listdir(INCLUDE)):
+        out.append(os.path.join(INCLUDE, name))
     return out
 
 
@@ -48,6 +52,7 @@ def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
     cu = [os.path.join(CSRC, n) for n in sorted(os.listdir(CSRC)) if n.endswith(".cu")]
+    cu += [os.path.join(HOST, n) for n in sorted(os.listdir(HOST)) if n.endswith(".cpp")]
     cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-shared", "-I", INCLUDE, "-I", CSRC, "-o", LIB + ".tmp"] + cu
     if verbose:
         print(" ".join(cmd))

@@ -81,6 +81,10 @@ struct DeviceGuard {
 
 namespace owl_detail {
 void set_error_literal(const char* msg) { g_lastLiteral = msg; }
+void set_error_string(const std::string& msg) {
+  g_lastLiteral = nullptr;
+  g_lastError = msg;
+}
 }  // namespace owl_detail
 
 struct owl_plan {

@@ -1,0 +1,61 @@
+/*
+ * owl_host.h -- C ABI of the host drivers above libowl: the reference's PRP and LL test loops
+ * (Gpu::isPrimePRP, src/Gpu.cpp:1400-1584; Gpu::isPrimeLL, src/Gpu.cpp:1586-1663) with their
+ * Gerbicz check, savefiles (src/Saver.cpp, formats "OWL PRP 13" / "OWL LL 13" with CRC32) and
+ * result residues, built in C++ on the engine calls of owl.h. Same status codes as owl.h.
+ */
+#ifndef OWL_HOST_H
+#define OWL_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  uint32_t block_size;    /* Gerbicz block B (reference -block; 1000 by default); divides 10000 */
+  uint32_t log_step;      /* res64 log/save step, a multiple of B (reference logStep, 20000) */
+  uint32_t check_step;    /* full-check interval, 0 = the reference's baseCheckStep(B) */
+  uint32_t stop_after;    /* 0 = run to the end; else stop at the first check point >= start + stop_after */
+  uint32_t n_savefiles;   /* savefiles kept (reference -save, 4) */
+  uint32_t W, H;          /* FFT shape, 0 = automatic */
+  const char* save_dir;   /* directory holding <E>/ (PRP) or ll-<E>/ (LL); NULL = no savefiles */
+  uint32_t inject_fault_k;/* test hook: flip one data word once after iteration k (0 = off) */
+  int verbose;            /* log lines to stderr */
+  uint32_t res_cap;       /* capacity of the checkpoint arrays below (may be 0) */
+  uint32_t* res_k;        /* iteration of each logged res64 */
+  uint64_t* res_res64;    /* data res64 at that iteration */
+  uint32_t* res_n;        /* number of checkpoints written */
+} owl_run_opts;
+
+typedef struct {
+  int is_prime;           /* PRP: 3^(2^E) == 9 (equals9, src/Gpu.cpp:1036); LL: final value 0 */
+  int finished;           /* the test reached its end (vs. stopped by stop_after) */
+  uint32_t k;             /* iteration reached */
+  uint64_t res64;         /* final: PRP type-1 residue 3^(2^E)/9 (doDiv9, src/Gpu.cpp:1128-1148); LL value */
+  uint32_t n_errors;      /* Gerbicz failures (each followed by a reload) */
+  char res2048[513];      /* PRP: first 64 words of the type-1 residue, hex, most significant first */
+} owl_run_result;
+
+/* PRP-3 test of 2^E - 1 (src/Gpu.cpp:1400-1584): resumes from save_dir/<E>/ when a savefile exists. */
+int owl_prp_run(int device, uint32_t E, const owl_run_opts* opts, owl_run_result* out);
+/* LL test of 2^E - 1 (src/Gpu.cpp:1586-1663): resumes from save_dir/ll-<E>/. */
+int owl_ll_run(int device, uint32_t E, const owl_run_opts* opts, owl_run_result* out);
+
+/* Savefile I/O on their own, for tools and tests (src/Saver.cpp:16-30, 86-143). check/data hold
+   nWords(E) = (E-1)/32+1 words. Return OWL_OK, or OWL_ERR_READ on a bad header or CRC. */
+int owl_prp_save(const char* save_dir, uint32_t E, uint32_t k, uint32_t block_size, uint64_t res64,
+                 const uint32_t* check, uint32_t n_errors, double elapsed);
+int owl_prp_load(const char* save_dir, uint32_t E, uint32_t* k, uint32_t* block_size, uint64_t* res64,
+                 uint32_t* check, uint32_t* n_errors, double* elapsed);
+int owl_ll_save(const char* save_dir, uint32_t E, uint32_t k, const uint32_t* data, double elapsed);
+int owl_ll_load(const char* save_dir, uint32_t E, uint32_t* k, uint32_t* data, double* elapsed);
+/* CRC-32 (IEEE 802.3, reflected), the savefile checksum (src/common.cpp crc32) */
+uint32_t owl_crc32(const void* data, size_t size);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -113,6 +113,7 @@ void pass1(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {
     case 64: p1w<64>(p, mode, F, words, flags); break;
     case 128: p1w<128>(p, mode, F, words, flags); break;
     case 256: p1w<256>(p, mode, F, words, flags); break;
+    case 512: p1w<512>(p, mode, F, words, flags); break;
     default: throw std::runtime_error("emu W");
   }
   if (mode == P1_OUT) {
