@@ -93,6 +93,10 @@ _SIGS = {
     "owl_ll_save": ([ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, _U32P, ctypes.c_double], ctypes.c_int),
     "owl_ll_load": ([ctypes.c_char_p, ctypes.c_uint32, _U32P, _U32P, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "owl_crc32": ([ctypes.c_void_p, ctypes.c_size_t], ctypes.c_uint32),
+    "owl_batch_create": ([ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(_P), ctypes.POINTER(_P)], ctypes.c_int),
+    "owl_batch_square": ([_P, ctypes.POINTER(_P), ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int),
+    "owl_batch_sync": ([_P], ctypes.c_int),
+    "owl_batch_destroy": ([_P], ctypes.c_int),
     "owl_profile_square": ([_P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), _U32P], ctypes.c_int),
 }
 
@@ -129,10 +133,18 @@ def n_words(E):
     return (E - 1) // 32 + 1
 
 
-def fft_choose(E, max_bpw=0.0):
+def fft_choose(E, max_bpw=0.0, tune=None):
+    """(N, W, H) for exponent E (reference FFTConfig::bestFit). With `tune`, a tune.json written by
+    gpuowl_b200.tune, the W x H split measured fastest for that N is used."""
     lib = load()
     N, W, H = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
     _check(lib.owl_fft_choose(E, max_bpw, ctypes.byref(N), ctypes.byref(W), ctypes.byref(H)))
+    if tune and os.path.exists(tune):
+        import json
+        with open(tune) as f:
+            t = json.load(f)
+        if str(N.value) in t:
+            return N.value, int(t[str(N.value)][0]), int(t[str(N.value)][1])
     return N.value, W.value, H.value
 
 
@@ -327,3 +339,33 @@ def ll_load(save_dir, E):
 def crc32(data):
     b = bytes(data)
     return load().owl_crc32(b, len(b))
+
+
+class Batch:
+    """Plans of one device squared together, one CUDA-graph launch per call (owl_batch_*)."""
+
+    def __init__(self, plans, device=0):
+        self.lib = load()
+        self.plans = list(plans)
+        arr = (_P * len(self.plans))(*[p.h for p in self.plans])
+        h = _P()
+        _check(self.lib.owl_batch_create(device, len(self.plans), arr, ctypes.byref(h)))
+        self.h = h
+
+    def square(self, bufs, n, ll=False):
+        arr = (_P * len(bufs))(*bufs)
+        _check(self.lib.owl_batch_square(self.h, arr, int(n), SQ_LL if ll else 0))
+
+    def sync(self):
+        _check(self.lib.owl_batch_sync(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _check(self.lib.owl_batch_destroy(self.h))
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -819,6 +819,131 @@ int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint
   });
 }
 
+}  // extern "C"
+
+struct owl_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<owl_plan*> plans;
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> joins;
+  struct Entry {
+    std::vector<int32_t*> bufs;
+    uint32_t n, flags;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Entry> graphs;
+};
+
+namespace {
+
+void batch_destroy(owl_batch* b) {
+  DeviceGuard dg(b->device);
+  if (b->stream) { cudaStreamSynchronize(b->stream); }
+  for (auto& g : b->graphs) { cudaGraphExecDestroy(g.exec); }
+  for (auto e : b->joins) { cudaEventDestroy(e); }
+  if (b->fork) { cudaEventDestroy(b->fork); }
+  if (b->done) { cudaEventDestroy(b->done); }
+  if (b->stream) { cudaStreamDestroy(b->stream); }
+  delete b;
+}
+
+cudaGraphExec_t batch_graph(owl_batch* b, int32_t* const* bufs, uint32_t n, uint32_t flags) {
+  std::vector<int32_t*> key(bufs, bufs + b->plans.size());
+  for (auto& g : b->graphs) {
+    if (g.n == n && g.flags == flags && g.bufs == key) { return g.exec; }
+  }
+  if (b->graphs.size() >= 4) {
+    cudaGraphExecDestroy(b->graphs.front().exec);
+    b->graphs.erase(b->graphs.begin());
+  }
+  cudaGraph_t graph = nullptr;
+  ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  try {
+    ck(cudaEventRecord(b->fork, b->stream), "fork");
+    for (size_t i = 0; i < b->plans.size(); ++i) {
+      owl_plan* p = b->plans[i];
+      ck(cudaStreamWaitEvent(p->stream, b->fork, 0), "fork wait");
+      enqueue_square(p, bufs[i], bufs[i], n, flags, false);
+      ck(cudaEventRecord(b->joins[i], p->stream), "join");
+      ck(cudaStreamWaitEvent(b->stream, b->joins[i], 0), "join wait");
+    }
+  } catch (...) {
+    cudaStreamEndCapture(b->stream, &graph);
+    if (graph) { cudaGraphDestroy(graph); }
+    throw;
+  }
+  ck(cudaStreamEndCapture(b->stream, &graph), "cudaStreamEndCapture");
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  ck(e, "cudaGraphInstantiate");
+  b->graphs.push_back({key, n, flags, exec});
+  return exec;
+}
+
+}  // namespace
+
+extern "C" {
+
+int owl_batch_create(int device, uint32_t count, owl_plan* const* plans, owl_batch** out) {
+  return guarded([&] {
+    if (!out || !plans || count == 0) { fail(OWL_ERR_ARG, "bad argument"); }
+    *out = nullptr;
+    for (uint32_t i = 0; i < count; ++i) {
+      check_plan(plans[i]);
+      if (plans[i]->device != device) { fail(OWL_ERR_ARG, "all plans of a batch must be on its device"); }
+    }
+    DeviceGuard dg(device);
+    std::unique_ptr<owl_batch, void (*)(owl_batch*)> b(new owl_batch(), batch_destroy);
+    b->device = device;
+    b->plans.assign(plans, plans + count);
+    ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "cudaEventCreate");
+    b->joins.resize(count);
+    for (auto& e : b->joins) { ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate"); }
+    *out = b.release();
+  });
+}
+
+int owl_batch_square(owl_batch* b, int32_t* const* bufs, uint32_t n, uint32_t flags) {
+  return guarded([&] {
+    if (!b || !bufs) { fail(OWL_ERR_ARG, "bad argument"); }
+    if (n == 0) { return; }
+    for (size_t i = 0; i < b->plans.size(); ++i) { check_buf(b->plans[i], bufs[i]); }
+    DeviceGuard dg(b->device);
+    // the batch starts after each plan's pending work, and each plan's later work after the batch
+    for (size_t i = 0; i < b->plans.size(); ++i) {
+      ck(cudaEventRecord(b->joins[i], b->plans[i]->stream), "record");
+      ck(cudaStreamWaitEvent(b->stream, b->joins[i], 0), "wait");
+    }
+    cudaGraphExec_t exec = batch_graph(b, bufs, n, flags & (OWL_SQ_LL | OWL_SQ_MUL3));
+    ck(cudaGraphLaunch(exec, b->stream), "cudaGraphLaunch");
+    ck(cudaEventRecord(b->done, b->stream), "record");
+    for (owl_plan* p : b->plans) {
+      ck(cudaStreamWaitEvent(p->stream, b->done, 0), "wait");
+      p->roePos = std::max(p->roePos, std::min(n, kRoeCap));
+    }
+  });
+}
+
+int owl_batch_sync(owl_batch* b) {
+  return guarded([&] {
+    if (!b) { fail(OWL_ERR_ARG, "null batch"); }
+    DeviceGuard dg(b->device);
+    ck(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
+    for (owl_plan* p : b->plans) { sync_and_check(p); }
+  });
+}
+
+int owl_batch_destroy(owl_batch* b) {
+  return guarded([&] {
+    if (!b) { fail(OWL_ERR_ARG, "null batch"); }
+    batch_destroy(b);
+  });
+}
+
 int owl_probe_wait_timeout(owl_plan* plan) {
   return guarded([&] {
     check_plan(plan);

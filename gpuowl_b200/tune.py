@@ -1,0 +1,108 @@
+"""Autotuner for FFT shapes (replaces the reference's -tune, src/tune.cpp:106-186, which times
+each FFT with Gpu::timePRP and writes tune.txt).
+
+    python -m gpuowl_b200.tune [--min-lg 13] [--max-lg 23] [--iters 200] [--out tune.txt]
+
+For every FFT size N = 2^lg it times each W x H split this build supports (W, H powers of two in
+[64, 4096], H/W in {1/2, 1, 2, 4}) with owl_profile_square (device time of the two passes per
+squaring, at an exponent of 18 bits per word), keeps the fastest split, and records its max
+round-off. Output:
+  - tune.txt in the reference's format, "%6.1f %14s # %u" = microseconds per iteration, shape,
+    largest exponent (src/TuneEntry.cpp:94-105), rows in increasing cost and exponent;
+  - tune.json, {"N": [W, H, us_per_iter, max_roe]}, read by fft_choose(..., tune=path).
+"""
+import argparse
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+
+def spec(W, H):
+    """The reference's W:M:H shape grammar, H = M * height (height 256, 512 or 1K) when possible."""
+    def k(n):
+        return "%dK" % (n // 1024) if n % 1024 == 0 else str(n)
+    for h in (1024, 512, 256):
+        if H % h == 0 and 2 <= H // h <= 16:
+            return "%s:%d:%s" % (k(W), H // h, k(h))
+    return "%s:1:%s" % (k(W), k(H))
+
+
+def candidates(lg):
+    hN = 1 << (lg - 1)
+    out = []
+    for w in (64, 128, 256, 512, 1024, 2048, 4096):
+        h = hN // w
+        if 64 <= h <= 4096 and w * h == hN and h in (w // 2, w, 2 * w, 4 * w):
+            out.append((w, h))
+    return out
+
+
+def next_odd_exponent(x):
+    x = int(x) | 1
+    return x
+
+
+def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True):
+    import numpy as np
+    import gpuowl_b200 as owl
+    from gpuowl_b200 import build
+    build.build()
+    rows = {}
+    for lg in range(min_lg, max_lg + 1):
+        N = 1 << lg
+        E = next_odd_exponent(N * max_bpw * 0.98)
+        best = None
+        for (W, H) in candidates(lg):
+            with owl.Plan(E, device=device, W=W, H=H) as p:
+                b = p.alloc()
+                rng = np.random.default_rng(lg)
+                w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
+                if E % 32:
+                    w[-1] &= (1 << (E % 32)) - 1
+                p.writeIn(b, w)
+                p.profile_square(b, 20)  # warm
+                p.readROE()
+                prof = p.profile_square(b, iters)
+                us = 1e3 * (prof["pass2"][0] + prof["pass1"][0] + prof["edge"][0]) / iters
+                roe = float(p.readROE().max())
+            if verbose:
+                print("N=%-9d %-14s %8.2f us/iter  max ROE %.4f" % (N, spec(W, H), us, roe), flush=True)
+            if best is None or us < best[2]:
+                best = (W, H, us, roe)
+        if best:
+            rows[N] = best
+    return rows
+
+
+def write(rows, max_bpw, out_txt, out_json):
+    lines, prev_cost = [], 0.0
+    for N in sorted(rows):
+        W, H, us, roe = rows[N]
+        cost = max(us, prev_cost)
+        prev_cost = cost
+        lines.append("%6.1f %14s # %u" % (cost, spec(W, H), int(N * max_bpw)))
+    with open(out_txt, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    with open(out_json, "w") as f:
+        json.dump({str(N): list(v) for N, v in rows.items()}, f, indent=1)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--min-lg", type=int, default=13)
+    ap.add_argument("--max-lg", type=int, default=23)
+    ap.add_argument("--iters", type=int, default=200)
+    ap.add_argument("--bpw", type=float, default=18.0)
+    ap.add_argument("--out", default="tune.txt")
+    ap.add_argument("--json", default="tune.json")
+    a = ap.parse_args()
+    rows = tune(a.min_lg, a.max_lg, a.iters, a.bpw)
+    write(rows, a.bpw, a.out, a.json)
+    print(open(a.out).read())
+
+
+if __name__ == "__main__":
+    main()

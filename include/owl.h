@@ -123,6 +123,18 @@ int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint
    timeout. Returns OWL_ERR_TIMEOUT (the expected outcome) and leaves the plan usable. */
 int owl_probe_wait_timeout(owl_plan* plan);
 
+/* Batches of exponents (BASELINE "batched uneven exponents"; the reference runs 1-4 independent
+   workers, each with its own in-order queue, src/main.cpp:111-118). A batch groups plans of one
+   device, each with its own exponent and FFT shape; owl_batch_square runs n squarings of every
+   plan's buffer as ONE CUDA-graph launch (one fork-join graph, a branch per plan, captured on
+   first use and cached), so that small FFTs of different exponents share the GPU. The call is
+   asynchronous; later calls on any of the plans are ordered after it. */
+typedef struct owl_batch owl_batch;
+int owl_batch_create(int device, uint32_t count, owl_plan* const* plans, owl_batch** out);
+int owl_batch_square(owl_batch* batch, int32_t* const* bufs, uint32_t n, uint32_t flags);
+int owl_batch_sync(owl_batch* batch);
+int owl_batch_destroy(owl_batch* batch);
+
 /* No counterpart in the reference (its host allocates every device buffer up front).
    n squarings (flags as for owl_square) of `words`, a device buffer of N = 2*W*H balanced int32
    digits on `device`, in place, queued on `stream` (a cudaStream_t; NULL is the legacy default

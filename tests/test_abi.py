@@ -68,3 +68,23 @@ def test_plan_without_device_reports_nodev(lib):
     with pytest.raises(g.OwlError) as e:
         g.Plan(86243)
     assert e.value.status == -5
+
+
+def test_tuner_shape_grammar_and_candidates():
+    from gpuowl_b200 import tune
+    assert tune.spec(2048, 2048) == "2K:2:1K"
+    assert tune.spec(256, 512) == "256:2:256"
+    assert tune.spec(64, 64) == "64:1:64"
+    assert (2048, 2048) in tune.candidates(23) and (1024, 4096) in tune.candidates(23)
+    for lg in range(13, 26):
+        for (w, h) in tune.candidates(lg):
+            assert 2 * w * h == 1 << lg
+
+
+def test_tune_file_format(tmp_path):
+    from gpuowl_b200 import tune
+    rows = {1 << 18: (256, 512, 21.3, 0.1), 1 << 23: (2048, 2048, 117.0, 0.03)}
+    tune.write(rows, 18.0, tmp_path / "tune.txt", tmp_path / "tune.json")
+    lines = open(tmp_path / "tune.txt").read().splitlines()
+    assert lines[0] == "%6.1f %14s # %u" % (21.3, "256:2:256", 4718592)
+    assert lines[1].split()[1] == "2K:2:1K"

@@ -213,3 +213,27 @@ def test_gerbicz_identity_and_injected_fault(owl, E):
         p.copy(check, saved)
         p.modMul(check, data)
         assert not p.isEqual(check, aux)
+
+
+def test_batch_of_uneven_exponents_matches_gmp(owl, oracle):
+    """Exponents with different FFT shapes squared as one graph launch, twice in a row."""
+    exps = [(1000003, 128, 256), (1999993, 256, 256), (4989349, 256, 512), (2302981, 256, 256),
+            (9000011, 512, 512), (500009, 128, 128)]
+    plans = [owl.Plan(E, W=W, H=H) for (E, W, H) in exps]
+    try:
+        bufs, starts = [], []
+        for p in plans:
+            b = p.alloc()
+            w = random_words(p.E, p.E + 11)
+            p.writeIn(b, w)
+            bufs.append(b)
+            starts.append(w)
+        with owl.Batch(plans) as batch:
+            batch.square(bufs, 17)
+            batch.square(bufs, 17)
+            batch.sync()
+        for p, b, w in zip(plans, bufs, starts):
+            assert np.array_equal(p.readOut(b), oracle.gmp_square(p.E, w, 34)), p.E
+    finally:
+        for p in plans:
+            p.close()
