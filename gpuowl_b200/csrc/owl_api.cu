@@ -164,6 +164,8 @@ template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, 
 }
 
 #define OWL_FOR_SIZES(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+// column heights: the powers of two, and 5 * 2^k (radix-5 middle stage) for the 5 * 2^m FFT lengths
+#define OWL_FOR_H_SIZES(X) OWL_FOR_SIZES(X) X(640) X(1280) X(2560)
 
 void set_attrs(uint32_t W, uint32_t H) {
   switch (W) {
@@ -185,7 +187,7 @@ void set_attrs(uint32_t W, uint32_t H) {
     setp2attr<n, owl::P2_FWD>();    \
     setp2attr<n, owl::P2_MUL>();    \
     break;
-    OWL_FOR_SIZES(CASE_H)
+    OWL_FOR_H_SIZES(CASE_H)
 #undef CASE_H
     default:
       fail(OWL_ERR_ARG, "unsupported H");
@@ -222,7 +224,7 @@ void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts = -1) {
   case n:                               \
     p2launch<n>(p, mode, F, Fb, Fq, ts); \
     break;
-    OWL_FOR_SIZES(CASE_H)
+    OWL_FOR_H_SIZES(CASE_H)
 #undef CASE_H
     default:
       fail(OWL_ERR_ARG, "unsupported H");
@@ -356,8 +358,8 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
     uint32_t N;
     if (owl_fft_choose(E, 0, &N, &W, &H) != OWL_OK) { fail(OWL_ERR_ARG, "no FFT shape for this exponent"); }
   }
-  if (!owl::is_pow2(W) || !owl::is_pow2(H) || W < 64 || W > 4096 || H < 64 || H > 4096) {
-    fail(OWL_ERR_ARG, "W and H must be powers of two in [64, 4096]");
+  if (!owl::shape_supported(W, H)) {
+    fail(OWL_ERR_ARG, "W must be a power of two in [64, 4096]; H a power of two in [64, 4096] or 640, 1280, 2560");
   }
   const uint32_t N = 2 * W * H;
   // below ~8 bits per word the sloppy carry-in of a line group can overflow a
@@ -518,17 +520,19 @@ int owl_device_info(int ordinal, char* name, size_t name_len, size_t* total_mem,
 int owl_fft_choose(uint32_t E, double max_bpw, uint32_t* N, uint32_t* W, uint32_t* H) {
   return guarded([&] {
     if (!N || !W || !H) { fail(OWL_ERR_ARG, "null output"); }
+    // FFT lengths in increasing order: 5 * 2^(lg-3) (between 2^(lg-1) and 2^lg), then 2^lg
     for (uint32_t lg = 13; lg <= 25; ++lg) {
-      uint32_t n = 1u << lg;
-      double lim = max_bpw > 0 ? max_bpw : kDefaultMaxBpw - 0.3 * ((double)lg - 18.0);
-      if ((double)E / n > lim) { continue; }
-      uint32_t w = 1u << ((lg - 1) / 2);
-      uint32_t h = (n / 2) / w;
-      if (w < 64 || h > 4096) { break; }
-      *N = n;
-      *W = w;
-      *H = h;
-      return;
+      for (int five = 1; five >= 0; --five) {
+        uint32_t n = five ? 5u << (lg - 3) : 1u << lg;
+        double lim = max_bpw > 0 ? max_bpw : kDefaultMaxBpw - 0.3 * (std::log2((double)n) - 18.0);
+        if ((double)E / n > lim) { continue; }
+        uint32_t w = 0, h = 0;
+        if (!owl::shape_for(n, &w, &h)) { continue; }
+        *N = n;
+        *W = w;
+        *H = h;
+        return;
+      }
     }
     fail(OWL_ERR_ARG, "exponent outside the supported FFT range");
   });

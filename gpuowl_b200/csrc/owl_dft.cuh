@@ -161,8 +161,35 @@ template <bool INV> __device__ __forceinline__ void dft16(C* v) {
   }
 }
 
+constexpr double kC51 = 0.30901699437494742410;   // cos(2 pi / 5)
+constexpr double kC52 = -0.80901699437494742410;  // cos(4 pi / 5)
+constexpr double kS51 = 0.95105651629515357212;   // sin(2 pi / 5)
+constexpr double kS52 = 0.58778525229247312917;   // sin(4 pi / 5)
+
+// 5-point DFT: with t1 = x1 + x4, t2 = x2 + x3, t3 = x1 - x4, t4 = x2 - x3,
+// X1,4 = x0 + c1 t1 + c2 t2 -/+ i (s1 t3 + s2 t4), X2,3 = x0 + c2 t1 + c1 t2 -/+ i (s2 t3 - s1 t4)
+// (signs of the i terms flipped for the inverse)
+template <bool INV> __device__ __forceinline__ void dft5(C* v) {
+  const C x0 = v[0];
+  const C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+  const C t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+  const C a1 = mk(x0.x + kC51 * t1.x + kC52 * t2.x, x0.y + kC51 * t1.y + kC52 * t2.y);
+  const C a2 = mk(x0.x + kC52 * t1.x + kC51 * t2.x, x0.y + kC52 * t1.y + kC51 * t2.y);
+  const C b1 = mk(kS51 * t3.x + kS52 * t4.x, kS51 * t3.y + kS52 * t4.y);
+  const C b2 = mk(kS52 * t3.x - kS51 * t4.x, kS52 * t3.y - kS51 * t4.y);
+  const C ib1 = INV ? cmulmi(b1) : cmuli(b1);
+  const C ib2 = INV ? cmulmi(b2) : cmuli(b2);
+  v[0] = cadd(x0, cadd(t1, t2));
+  v[1] = csub(a1, ib1);
+  v[4] = cadd(a1, ib1);
+  v[2] = csub(a2, ib2);
+  v[3] = cadd(a2, ib2);
+}
+
 template <int R, bool INV> __device__ __forceinline__ void dftR(C* v) {
-  if constexpr (R == 2) {
+  if constexpr (R == 5) {
+    dft5<INV>(v);
+  } else if constexpr (R == 2) {
     dft2<INV>(v);
   } else if constexpr (R == 4) {
     dft4<INV>(v);
@@ -184,10 +211,20 @@ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x / 2); }
 // runs butterflies j = tl + (N/16) b, b < 16/R, inputs x[j + r N/R],
 // twiddle w_(NS R)^(r (j mod NS)), outputs y[(j/NS) NS R + j mod NS + r NS].
 
+// butterflies per thread of a radix-R stage (radix 5 leaves the last one to some threads only)
+template <int R> constexpr int st_nb() { return (16 + R - 1) / R; }
+template <int R, int N> __device__ __forceinline__ bool st_has(int j) { return (16 % R == 0) || j < N / R; }
+// j mod NS and j / NS for j >= 0 (mask and shift when NS is a power of two)
+template <int NS> __device__ __forceinline__ int smod(int j) {
+  if constexpr ((NS & (NS - 1)) == 0) { return j & (NS - 1); } else { return (int)((unsigned)j % (unsigned)NS); }
+}
+template <int NS> __device__ __forceinline__ int sdiv(int j) { return (int)((unsigned)j / (unsigned)NS); }
+
 template <int R, int N, int PS> __device__ __forceinline__ void st_load(const C* buf, int tl, C* v) {
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < st_nb<R>(); ++b) {
     int j = tl + (N / 16) * b;
+    if (!st_has<R, N>(j)) { continue; }
 #pragma unroll
     for (int r = 0; r < R; ++r) { v[b * R + r] = buf[pad<PS>(j + r * (N / R))]; }
   }
@@ -202,9 +239,10 @@ template <bool INV> __device__ __forceinline__ void twmul(C& v, C w) { v = cmulw
 template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twiddle(int tl, C* v, const C* __restrict__ tab) {
   if constexpr (NS > 1) {
 #pragma unroll
-    for (int b = 0; b < 16 / R; ++b) {
+    for (int b = 0; b < st_nb<R>(); ++b) {
       int j = tl + (N / 16) * b;
-      int k = j & (NS - 1);
+      if (!st_has<R, N>(j)) { continue; }
+      int k = smod<NS>(j);
       C* x = v + b * R;
       if constexpr (R >= 8) {
         const C w1 = __ldg(tab + 1 * NS + k);
@@ -240,14 +278,15 @@ template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twi
 
 template <int R, bool INV> __device__ __forceinline__ void st_dft(C* v) {
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) { dftR<R, INV>(v + b * R); }
+  for (int b = 0; b < st_nb<R>(); ++b) { dftR<R, INV>(v + b * R); }
 }
 
 template <int R, int N, int NS, int PS> __device__ __forceinline__ void st_store(C* buf, int tl, const C* v) {
 #pragma unroll
-  for (int b = 0; b < 16 / R; ++b) {
+  for (int b = 0; b < st_nb<R>(); ++b) {
     int j = tl + (N / 16) * b;
-    int base = (j / NS) * NS * R + (j & (NS - 1));
+    if (!st_has<R, N>(j)) { continue; }
+    int base = sdiv<NS>(j) * NS * R + smod<NS>(j);
 #pragma unroll
     for (int r = 0; r < R; ++r) { buf[pad<PS>(base + r * NS)] = v[b * R + r]; }
   }
@@ -256,9 +295,13 @@ template <int R, int N, int NS, int PS> __device__ __forceinline__ void st_store
 // Radix plan for a line of N points whose last inverse / first forward stage
 // (radix RL) is split across lines or columns: N = R1 * M1 * M2 * RL.
 // "A order" runs the stages R1, M1, M2, RL; "B order" runs RL, M2, M1, R1.
+// n = 2^a or 5 * 2^a; the factor 5 becomes the M2 stage
 constexpr int plan_r1(int n, int rl) { return n / rl >= 16 ? 16 : n / rl; }
-constexpr int plan_m1(int n, int rl) { return (n / rl / plan_r1(n, rl)) >= 16 ? 16 : n / rl / plan_r1(n, rl); }
-constexpr int plan_m2(int n, int rl) { return n / rl / plan_r1(n, rl) / plan_m1(n, rl); }
+constexpr int plan_rest2(int n, int rl) { return n / rl / plan_r1(n, rl); }
+constexpr int plan_m1(int n, int rl) {
+  return plan_rest2(n, rl) % 5 == 0 ? plan_rest2(n, rl) / 5 : (plan_rest2(n, rl) >= 16 ? 16 : plan_rest2(n, rl));
+}
+constexpr int plan_m2(int n, int rl) { return plan_rest2(n, rl) / plan_m1(n, rl); }
 
 // Stage twiddle tables, one per stage with twiddles, each laid out [r][k]:
 // entry r * NS + k = w_(R NS)^(r k) (forward sign), so that a warp's threads
@@ -286,6 +329,8 @@ template <int N, int RL> struct Plan {
   static constexpr TwOffsets TW = tw_offsets(N, RL);
   static_assert(R1 * M1 * M2 * RL == N, "plan");
   static_assert(M2 >= 1 && M2 <= 16, "plan depth");
+  static_assert(M1 <= 16 && (16 % M1 == 0), "plan: first middle radix must divide 16");
+  static_assert(M2 == 5 || (16 % M2 == 0), "plan: second middle radix 5 or a divisor of 16");
   static_assert(R1 >= 4, "first radix too small for conflict-free padding");
 };
 

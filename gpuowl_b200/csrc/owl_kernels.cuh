@@ -145,7 +145,7 @@ template <int W, int R> __device__ __forceinline__ void p1_fwd_first(C* ln, int 
 // ---------------------------------------------------------------------------
 // Pass 1: R lines of W points per CTA, R*W/16 threads, 16 values per thread.
 template <int W, int R, int MODE>
-__global__ void __launch_bounds__(R * W / 16, (R * W / 16 >= 256) ? 2 : 1)
+__global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
     k_pass1(Args a, C* __restrict__ F, int32_t* __restrict__ words, int roeSlot, int flags, int tslot) {
   constexpr int T = R * W / 16;
   constexpr int RL = 16 / R;
@@ -518,7 +518,7 @@ __device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
 }
 
 template <int H, int R, int MODE>
-__global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
+__global__ void __launch_bounds__(H / 8, (H / 8 == 256) ? 2 : 1)
     k_pass2(Args a, C* __restrict__ F, const C* __restrict__ Fb, C* __restrict__ Fq, int tslot) {
   constexpr int T = H / 8;
   constexpr int TC = H / 16;  // threads per column in the per-column stages
@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
   }
   __syncthreads();
 
-  C u[16];
+  C u[20];  // 16 values per thread; a radix-5 stage runs up to 4 butterflies
   // ---- forward column DFT, first stage from HBM with the w_hN^(k1 j2) twiddle ----
 #pragma unroll
   for (int b = 0; b < 16 / P::R1; ++b) {
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(H / 8, (H / 8 >= 256) ? 2 : 1)
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
         uint32_t kA2 = t + T * r;
-        uint32_t pA = (H - kA2) & (H - 1);
+        uint32_t pA = (kA2 == 0) ? 0u : H - kA2;
         uint32_t kB2 = jB + T * r;
         uint32_t pB = H - 1 - kB2;
         C t2A = mul_w8<false>(baseA, r);

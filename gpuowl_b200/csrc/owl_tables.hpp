@@ -87,8 +87,43 @@ struct Tables {
 // lines per pass-1 block; the width FFT's cross-line radix is 16 / kLinesPerBlock
 constexpr uint32_t kLinesPerBlock = 2;
 
+// Shapes this build supports: W a power of two in [64, 4096]; H a power of two in
+// [64, 4096], or 5 * 2^k in {640, 1280, 2560} (a radix-5 stage in the column FFT).
+inline bool h_supported(uint32_t H) {
+  return (is_pow2(H) && H >= 64 && H <= 4096) || H == 640 || H == 1280 || H == 2560;
+}
+inline bool shape_supported(uint32_t W, uint32_t H) { return is_pow2(W) && W >= 64 && W <= 4096 && h_supported(H); }
+
+// The default W x H split of an FFT of n words: for 2^lg, W = 2^((lg-1)/2) <= H;
+// for 5 * 2^k the supported H that makes the shape closest to square (ties to the larger H).
+inline bool shape_for(uint32_t n, uint32_t* W, uint32_t* H) {
+  const uint32_t hN = n / 2;
+  if (is_pow2(n)) {
+    const uint32_t w = 1u << ((log2u(n) - 1) / 2), h = hN / w;
+    if (!shape_supported(w, h)) { return false; }
+    *W = w;
+    *H = h;
+    return true;
+  }
+  bool found = false;
+  double best = 0;
+  for (uint32_t h : {2560u, 1280u, 640u}) {
+    if (hN % h) { continue; }
+    const uint32_t w = hN / h;
+    if (!shape_supported(w, h)) { continue; }
+    const double d = std::fabs(std::log((double)w / h));
+    if (!found || d < best - 1e-9) {
+      found = true;
+      best = d;
+      *W = w;
+      *H = h;
+    }
+  }
+  return found;
+}
+
 inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
-  if (!is_pow2(W) || !is_pow2(H)) { throw std::invalid_argument("W and H must be powers of two"); }
+  if (!shape_supported(W, H)) { throw std::invalid_argument("unsupported W x H shape"); }
   Tables t;
   t.E = E;
   t.W = W;
@@ -129,23 +164,6 @@ inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
     t.iwt2[i] = (double)(exp2l(-(long double)X / N) * norm);
   }
   return t;
-}
-
-// Shapes this build supports: W, H powers of two in [64, 4096], H >= W.
-// Smallest N = 2 W H whose bits per word E/N stays at or below `maxBpw`.
-inline bool choose_shape(uint32_t E, double maxBpw, uint32_t* W, uint32_t* H) {
-  for (uint32_t lg = 13; lg <= 25; ++lg) {
-    uint32_t N = 1u << lg;
-    if ((double)E / N > maxBpw) { continue; }
-    uint32_t hN = N / 2;
-    uint32_t w = 1u << ((lg - 1) / 2);
-    uint32_t h = hN / w;
-    if (w < 64 || h > 4096) { return false; }
-    *W = w;
-    *H = h;
-    return true;
-  }
-  return false;
 }
 
 }  // namespace owl

@@ -3,8 +3,9 @@ each FFT with Gpu::timePRP and writes tune.txt).
 
     python -m gpuowl_b200.tune [--min-lg 13] [--max-lg 23] [--iters 200] [--out tune.txt]
 
-For every FFT size N = 2^lg it times each W x H split this build supports (W, H powers of two in
-[64, 4096], H/W in {1/2, 1, 2, 4}) with owl_profile_square (device time of the two passes per
+For every FFT size N = 2^lg, and N = 5 * 2^(lg-3) with --five, it times each W x H split this build
+supports (W a power of two in [64, 4096]; H a power of two in [64, 4096] with H/W in {1/2, 1, 2, 4},
+or H in {640, 1280, 2560}) with owl_profile_square (device time of the two passes per
 squaring, at an exponent of 18 bits per word), keeps the fastest split, and records its max
 round-off. Output:
   - tune.txt in the reference's format, "%6.1f %14s # %u" = microseconds per iteration, shape,
@@ -30,13 +31,24 @@ def spec(W, H):
     return "%s:1:%s" % (k(W), k(H))
 
 
-def candidates(lg):
-    hN = 1 << (lg - 1)
+def candidates(N):
+    hN = N // 2
     out = []
     for w in (64, 128, 256, 512, 1024, 2048, 4096):
         h = hN // w
-        if 64 <= h <= 4096 and w * h == hN and h in (w // 2, w, 2 * w, 4 * w):
+        if w * h != hN:
+            continue
+        if h in (640, 1280, 2560) or (64 <= h <= 4096 and h in (w // 2, w, 2 * w, 4 * w)):
             out.append((w, h))
+    return out
+
+
+def sizes(min_lg, max_lg, five):
+    out = []
+    for lg in range(min_lg, max_lg + 1):
+        if five and lg >= 3:
+            out.append(5 << (lg - 3))
+        out.append(1 << lg)
     return out
 
 
@@ -45,20 +57,19 @@ def next_odd_exponent(x):
     return x
 
 
-def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True):
+def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True, five=False):
     import numpy as np
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
     build.build()
     rows = {}
-    for lg in range(min_lg, max_lg + 1):
-        N = 1 << lg
+    for N in sizes(min_lg, max_lg, five):
         E = next_odd_exponent(N * max_bpw * 0.98)
         best = None
-        for (W, H) in candidates(lg):
+        for (W, H) in candidates(N):
             with owl.Plan(E, device=device, W=W, H=H) as p:
                 b = p.alloc()
-                rng = np.random.default_rng(lg)
+                rng = np.random.default_rng(N)
                 w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
                 if E % 32:
                     w[-1] &= (1 << (E % 32)) - 1
@@ -98,8 +109,9 @@ def main():
     ap.add_argument("--bpw", type=float, default=18.0)
     ap.add_argument("--out", default="tune.txt")
     ap.add_argument("--json", default="tune.json")
+    ap.add_argument("--five", action="store_true", help="also the 5 * 2^k FFT lengths")
     a = ap.parse_args()
-    rows = tune(a.min_lg, a.max_lg, a.iters, a.bpw)
+    rows = tune(a.min_lg, a.max_lg, a.iters, a.bpw, five=a.five)
     write(rows, a.bpw, a.out, a.json)
     print(open(a.out).read())
 

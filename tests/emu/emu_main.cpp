@@ -128,6 +128,8 @@ void pass2(EmuPlan& p, int mode, C* F, const C* Fb, C* Fq) {
     case 128: p2h<128>(p, mode, F, Fb, Fq); break;
     case 256: p2h<256>(p, mode, F, Fb, Fq); break;
     case 512: p2h<512>(p, mode, F, Fb, Fq); break;
+    case 640: p2h<640>(p, mode, F, Fb, Fq); break;
+    case 1280: p2h<1280>(p, mode, F, Fb, Fq); break;
     default: throw std::runtime_error("emu H");
   }
 }

@@ -57,6 +57,8 @@ def test_fft_choice_matches_the_configs(lib):
     import gpuowl_b200 as g
     assert g.fft_choose(4989349) == (262144, 256, 512)        # 256K (reference 256:2:256)
     assert g.fft_choose(136181029) == (8388608, 2048, 2048)   # 8M  (reference 1K:8:512)
+    assert g.fft_choose(333000017) == (20971520, 4096, 2560)  # 20M = 5 * 2^22 (reference 4K:5:512)
+    assert g.fft_choose(40000003) == (5 << 19, 1024, 1280)   # 2.5M, between 2M and 4M
     with pytest.raises(g.OwlError):
         g.fft_choose(3_000_000_000)
 
@@ -75,10 +77,12 @@ def test_tuner_shape_grammar_and_candidates():
     assert tune.spec(2048, 2048) == "2K:2:1K"
     assert tune.spec(256, 512) == "256:2:256"
     assert tune.spec(64, 64) == "64:1:64"
-    assert (2048, 2048) in tune.candidates(23) and (1024, 4096) in tune.candidates(23)
-    for lg in range(13, 26):
-        for (w, h) in tune.candidates(lg):
-            assert 2 * w * h == 1 << lg
+    assert tune.spec(4096, 2560) == "4K:5:512"
+    assert (2048, 2048) in tune.candidates(1 << 23) and (1024, 4096) in tune.candidates(1 << 23)
+    assert (4096, 2560) in tune.candidates(5 << 22)
+    for N in tune.sizes(13, 25, five=True):
+        for (w, h) in tune.candidates(N):
+            assert 2 * w * h == N
 
 
 def test_tune_file_format(tmp_path):

@@ -47,6 +47,7 @@ def run(exe, *args):
     (86243, 64, 64, 40, 2),       # LL from 4
     (110503, 64, 64, 30, 1),      # MUL3 on the last step
     (500009, 128, 128, 24, 0),    # radix-16 first stages, two-level twiddles
+    (1300021, 64, 640, 4, 2),     # H = 5 * 128: radix-5 middle stage of the column FFT, LL
 ])
 def test_emulated_square_matches_gmp(emu, oracle, E, W, H, n, flags):
     roe, got = run(emu, "square", E, W, H, n, flags, 0)
@@ -64,3 +65,30 @@ def test_emulated_modmul_matches_gmp(emu, oracle, mul3):
     roe, got = run(emu, "modmul", E, 64, 64, mul3, 11, 22)
     want = oracle.gmp_mul(E, random_words(E, 11), random_words(E, 22), mul3=bool(mul3))
     assert np.array_equal(got, want)
+
+
+def splitmix_words(E, seed):
+    """The emulator's random start (splitmix64 stream, one word per draw, top word masked to E bits)."""
+    m = (1 << 64) - 1
+    s, out = seed, []
+    for _ in range((E - 1) // 32 + 1):
+        s = (s + 0x9e3779b97f4a7c15) & m
+        z = s
+        z = ((z ^ (z >> 30)) * 0xbf58476d1ce4e5b9) & m
+        z = ((z ^ (z >> 27)) * 0x94d049bb133111eb) & m
+        out.append((z ^ (z >> 31)) & 0xffffffff)
+    w = np.array(out, dtype=np.uint32)
+    if E % 32:
+        w[-1] &= (1 << (E % 32)) - 1
+    return w
+
+
+@pytest.mark.parametrize("E,W,H,n,seed", [
+    (1300021, 64, 640, 3, 7),     # 5 * 2^14 words, radix plan 16 * 5 * 8
+    (2500009, 64, 1280, 2, 9),    # 5 * 2^15 words, radix plan 16 * 2 * 5 * 8
+])
+def test_emulated_radix5_random_start(emu, oracle, E, W, H, n, seed):
+    roe, got = run(emu, "square", E, W, H, n, 0, seed)
+    want = oracle.gmp_square(E, splitmix_words(E, seed), n)
+    assert np.array_equal(got, want)
+    assert 0 < roe < 0.1

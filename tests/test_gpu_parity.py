@@ -45,6 +45,29 @@ def test_square_large_shapes_vs_gmp(owl, oracle, E, W, H):
     assert np.array_equal(got, want)
 
 
+# 5 * 2^k FFT lengths (radix-5 middle stage of the column FFT, H = 640, 1280, 2560) and the
+# 512-thread 4096-point instantiations, up to the 20M (5 * 2^22) and 32M lengths
+SHAPES_WIDE = [
+    (1300021, 64, 640), (2500009, 64, 1280), (20000003, 1024, 640), (40000003, 1024, 1280),
+    (80000023, 2048, 1280), (270000017, 2048, 4096), (333000017, 4096, 2560), (536000009, 4096, 4096),
+]
+
+
+@pytest.mark.parametrize("E,W,H", SHAPES_WIDE)
+def test_square_radix5_and_4k_shapes_vs_gmp(owl, oracle, E, W, H):
+    n = 4
+    with owl.Plan(E, W=W, H=H) as p:
+        start = random_words(E, E + 11)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.squareLoop(a, a, n)
+        got = p.readOut(a)
+        roe = float(p.readROE().max())
+    want = oracle.gmp_square(E, start, n)
+    assert np.array_equal(got, want)
+    assert roe < 0.3
+
+
 @pytest.mark.parametrize("E,W,H", [SHAPES[0], SHAPES[3], SHAPES[5], SHAPES[8]])
 def test_mul3_last(owl, oracle, E, W, H):
     """squareLoop with doTailMul3: the last squaring is multiplied by 3 (Gerbicz aux)."""
@@ -59,7 +82,7 @@ def test_mul3_last(owl, oracle, E, W, H):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("E,W,H", [SHAPES[0], SHAPES[2], SHAPES[5], SHAPES[8], SHAPES[10]])
+@pytest.mark.parametrize("E,W,H", [SHAPES[0], SHAPES[2], SHAPES[5], SHAPES[8], SHAPES[10], SHAPES_WIDE[2]])
 @pytest.mark.parametrize("mul3", [False, True])
 def test_modmul_vs_gmp(owl, oracle, E, W, H, mul3):
     with owl.Plan(E, W=W, H=H) as p:
