@@ -45,7 +45,8 @@ class RunOpts(ctypes.Structure):
                 ("stop_after", ctypes.c_uint32), ("n_savefiles", ctypes.c_uint32), ("W", ctypes.c_uint32),
                 ("H", ctypes.c_uint32), ("save_dir", ctypes.c_char_p), ("inject_fault_k", ctypes.c_uint32),
                 ("verbose", ctypes.c_int), ("res_cap", ctypes.c_uint32), ("res_k", ctypes.POINTER(ctypes.c_uint32)),
-                ("res_res64", ctypes.POINTER(ctypes.c_uint64)), ("res_n", ctypes.POINTER(ctypes.c_uint32))]
+                ("res_res64", ctypes.POINTER(ctypes.c_uint64)), ("res_n", ctypes.POINTER(ctypes.c_uint32)),
+                ("split", ctypes.c_int)]
 
 
 class RunResult(ctypes.Structure):
@@ -67,6 +68,7 @@ _SIGS = {
     "owl_plan_destroy": ([_P], ctypes.c_int),
     "owl_plan_shape": ([_P, _U32P, _U32P, _U32P], ctypes.c_int),
     "owl_plan_set_timeout": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "owl_plan_set_split": ([_P, ctypes.c_int], ctypes.c_int),
     "owl_buf_alloc": ([_P, ctypes.POINTER(_P)], ctypes.c_int),
     "owl_buf_free": ([_P, _P], ctypes.c_int),
     "owl_buf_copy": ([_P, _P, _P], ctypes.c_int),
@@ -162,7 +164,7 @@ class Plan:
     balanced int32 digits in natural word order.
     """
 
-    def __init__(self, E, device=0, W=0, H=0):
+    def __init__(self, E, device=0, W=0, H=0, split=False):
         self.lib = load()
         self.E = int(E)
         self.device = device
@@ -173,6 +175,9 @@ class Plan:
         _check(self.lib.owl_plan_shape(self.h, ctypes.byref(N), ctypes.byref(Wv), ctypes.byref(Hv)))
         self.N, self.W, self.H = N.value, Wv.value, Hv.value
         self.nwords = n_words(self.E)
+        self.split = False
+        if split:
+            self.set_split(True)
 
     def close(self):
         if getattr(self, "h", None):
@@ -208,6 +213,12 @@ class Plan:
 
     def set_timeout(self, ns):
         _check(self.lib.owl_plan_set_timeout(self.h, int(ns)))
+
+    def set_split(self, enable=True):
+        """Split-precision column pass: INT8 tensor-core GEMMs for the first forward and last
+        inverse 32-point stages of every column FFT (H = 2048 only)."""
+        _check(self.lib.owl_plan_set_split(self.h, 1 if enable else 0))
+        self.split = bool(enable)
 
     def write_digits(self, buf, digits):
         d = np.ascontiguousarray(digits, dtype=np.int32)
@@ -283,14 +294,14 @@ class Plan:
 # ---- host drivers (include/owl_host.h) ----
 
 def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, W, H, inject_fault_k, verbose,
-         n_savefiles=4, cap=4096):
+         n_savefiles=4, cap=4096, split=False):
     lib = load()
     ks = (ctypes.c_uint32 * cap)()
     rs = (ctypes.c_uint64 * cap)()
     n = ctypes.c_uint32(0)
     o = RunOpts(block, log_step, check_step, stop_after, n_savefiles, W, H,
                 save_dir.encode() if save_dir else None, inject_fault_k, 1 if verbose else 0, cap,
-                ks, rs, ctypes.pointer(n))
+                ks, rs, ctypes.pointer(n), 1 if split else 0)
     r = RunResult()
     _check(getattr(lib, fn_name)(device, E, ctypes.byref(o), ctypes.byref(r)))
     return {"is_prime": bool(r.is_prime), "finished": bool(r.finished), "k": r.k, "res64": r.res64,
@@ -299,15 +310,15 @@ def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, 
 
 
 def prp_run(E, device=0, block=1000, log_step=20000, check_step=0, stop_after=0, save_dir=None, W=0, H=0,
-            inject_fault_k=0, verbose=False):
+            inject_fault_k=0, verbose=False, split=False):
     """PRP-3 test (the reference's Gpu::isPrimePRP) through owl_prp_run."""
     return _run("owl_prp_run", E, device, block, log_step, check_step, stop_after, save_dir, W, H,
-                inject_fault_k, verbose)
+                inject_fault_k, verbose, split=split)
 
 
-def ll_run(E, device=0, log_step=10000, stop_after=0, save_dir=None, W=0, H=0, verbose=False):
+def ll_run(E, device=0, log_step=10000, stop_after=0, save_dir=None, W=0, H=0, verbose=False, split=False):
     """Lucas-Lehmer test (the reference's Gpu::isPrimeLL) through owl_ll_run."""
-    return _run("owl_ll_run", E, device, 1000, log_step, 0, stop_after, save_dir, W, H, 0, verbose)
+    return _run("owl_ll_run", E, device, 1000, log_step, 0, stop_after, save_dir, W, H, 0, verbose, split=split)
 
 
 def prp_save(save_dir, E, k, block, res64, check, n_errors=0, elapsed=0.0):

@@ -18,6 +18,7 @@
 
 #include "owl.h"
 #include "owl_kernels.cuh"
+#include "owl_pass2_tc.cuh"
 #include "owl_tables.hpp"
 #include "owl_words.hpp"
 
@@ -112,6 +113,10 @@ struct owl_plan {
   };
   std::vector<GraphEntry> graphs;
   uint64_t useClock = 0;
+  // split-precision column pass (H = 2048 only): DFT digit planes and its stage tables
+  bool split = false;
+  const unsigned char* tcB = nullptr;
+  const C* twHtc = nullptr;
 };
 
 namespace {
@@ -127,6 +132,27 @@ template <int H, int M> void setp2attr() {
   size_t sm = 2 * (size_t)owl::p2_col_stride<H>() * sizeof(C);
   ck(cudaFuncSetAttribute(owl::k_pass2<H, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
      "cudaFuncSetAttribute(pass2)");
+}
+
+template <int M> void setp2tcattr() {
+  ck(cudaFuncSetAttribute(owl::k_pass2_tc<kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, owl::kTcSmem),
+     "cudaFuncSetAttribute(pass2 split)");
+}
+
+void p2launch_tc(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts) {
+  dim3 grid(p->W / 2);
+  constexpr int T = owl::kTcH / 8;
+  switch (mode) {
+    case owl::P2_SQUARE:
+      owl::k_pass2_tc<kR, owl::P2_SQUARE><<<grid, T, owl::kTcSmem, p->stream>>>(p->args, p->tcB, p->twHtc, F, Fb, Fq, ts);
+      break;
+    case owl::P2_FWD:
+      owl::k_pass2_tc<kR, owl::P2_FWD><<<grid, T, owl::kTcSmem, p->stream>>>(p->args, p->tcB, p->twHtc, F, Fb, Fq, ts);
+      break;
+    default:
+      owl::k_pass2_tc<kR, owl::P2_MUL><<<grid, T, owl::kTcSmem, p->stream>>>(p->args, p->tcB, p->twHtc, F, Fb, Fq, ts);
+      break;
+  }
 }
 
 template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags, int ts) {
@@ -192,6 +218,11 @@ void set_attrs(uint32_t W, uint32_t H) {
     default:
       fail(OWL_ERR_ARG, "unsupported H");
   }
+  if (H == (uint32_t)owl::kTcH) {
+    setp2tcattr<owl::P2_SQUARE>();
+    setp2tcattr<owl::P2_FWD>();
+    setp2tcattr<owl::P2_MUL>();
+  }
 }
 
 void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot = -1, int ts = -1) {
@@ -219,6 +250,11 @@ void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot
 }
 
 void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts = -1) {
+  if (p->split) {
+    p2launch_tc(p, mode, F, Fb, Fq, ts);
+    ck(cudaGetLastError(), "pass2 split launch");
+    return;
+  }
   switch (p->H) {
 #define CASE_H(n)                       \
   case n:                               \
@@ -381,9 +417,12 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
 
   // tables: one allocation
   static_assert(kR == owl::kLinesPerBlock, "table layout and launch disagree on lines per block");
-  size_t nC = t.twW.size() + t.twH.size() + t.rootH.size() + t.twLo.size() + t.twHi.size();
-  size_t bytes = 256 * 13 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
-                 (t.x1.size() + t.x2.size()) * sizeof(uint32_t);
+  const bool tcShape = (H == (uint32_t)owl::kTcH);
+  const std::vector<owl::HostC> twHtc = tcShape ? owl::stage_tables(H, 8, owl::kTcR1) : std::vector<owl::HostC>();
+  const std::vector<uint8_t> tcB = tcShape ? owl::tc_dft_digits() : std::vector<uint8_t>();
+  size_t nC = t.twW.size() + t.twH.size() + t.rootH.size() + t.twLo.size() + t.twHi.size() + twHtc.size();
+  size_t bytes = 256 * 15 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
+                 (t.x1.size() + t.x2.size()) * sizeof(uint32_t) + tcB.size();
   ck(cudaMalloc(&p->tableMem, bytes), "cudaMalloc(tables)");
   std::vector<char> host(bytes, 0);
   char* hcur = host.data();
@@ -405,6 +444,10 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   p->args.wt2 = reinterpret_cast<const double*>(dbase + put(t.wt2.data(), t.wt2.size() * sizeof(double)));
   p->args.iwt2 = reinterpret_cast<const double*>(dbase + put(t.iwt2.data(), t.iwt2.size() * sizeof(double)));
   p->args.x2 = reinterpret_cast<const uint32_t*>(dbase + put(t.x2.data(), t.x2.size() * sizeof(uint32_t)));
+  if (tcShape) {
+    p->twHtc = reinterpret_cast<const C*>(dbase + put(twHtc.data(), twHtc.size() * sizeof(C)));
+    p->tcB = reinterpret_cast<const unsigned char*>(dbase + put(tcB.data(), tcB.size()));
+  }
   ck(cudaMemcpy(p->tableMem, host.data(), bytes, cudaMemcpyHostToDevice), "upload tables");
 
   // FFT work buffers
@@ -563,6 +606,20 @@ int owl_plan_set_timeout(owl_plan* plan, uint64_t ns) {
     check_plan(plan);
     if (ns == 0) { fail(OWL_ERR_ARG, "timeout must be positive"); }
     plan->args.timeoutNs = ns;
+  });
+}
+
+int owl_plan_set_split(owl_plan* plan, int enable) {
+  return guarded([&] {
+    check_plan(plan);
+    if (enable && plan->H != (uint32_t)owl::kTcH) {
+      fail(OWL_ERR_ARG, "the split-precision column pass needs H = 2048");
+    }
+    DeviceGuard dg(plan->device);
+    ck(cudaStreamSynchronize(plan->stream), "cudaStreamSynchronize");
+    for (auto& g : plan->graphs) { cudaGraphExecDestroy(g.exec); }
+    plan->graphs.clear();
+    plan->split = enable != 0;
   });
 }
 

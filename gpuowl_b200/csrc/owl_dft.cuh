@@ -295,13 +295,15 @@ template <int R, int N, int NS, int PS> __device__ __forceinline__ void st_store
 // Radix plan for a line of N points whose last inverse / first forward stage
 // (radix RL) is split across lines or columns: N = R1 * M1 * M2 * RL.
 // "A order" runs the stages R1, M1, M2, RL; "B order" runs RL, M2, M1, R1.
-// n = 2^a or 5 * 2^a; the factor 5 becomes the M2 stage
-constexpr int plan_r1(int n, int rl) { return n / rl >= 16 ? 16 : n / rl; }
-constexpr int plan_rest2(int n, int rl) { return n / rl / plan_r1(n, rl); }
-constexpr int plan_m1(int n, int rl) {
-  return plan_rest2(n, rl) % 5 == 0 ? plan_rest2(n, rl) / 5 : (plan_rest2(n, rl) >= 16 ? 16 : plan_rest2(n, rl));
+// n = 2^a or 5 * 2^a; the factor 5 becomes the M2 stage. r1f != 0 forces the
+// first radix (the split-precision column pass runs a 32-point first stage).
+constexpr int plan_r1(int n, int rl, int r1f = 0) { return r1f ? r1f : (n / rl >= 16 ? 16 : n / rl); }
+constexpr int plan_rest2(int n, int rl, int r1f = 0) { return n / rl / plan_r1(n, rl, r1f); }
+constexpr int plan_m1(int n, int rl, int r1f = 0) {
+  return plan_rest2(n, rl, r1f) % 5 == 0 ? plan_rest2(n, rl, r1f) / 5
+                                          : (plan_rest2(n, rl, r1f) >= 16 ? 16 : plan_rest2(n, rl, r1f));
 }
-constexpr int plan_m2(int n, int rl) { return plan_rest2(n, rl) / plan_m1(n, rl); }
+constexpr int plan_m2(int n, int rl, int r1f = 0) { return plan_rest2(n, rl, r1f) / plan_m1(n, rl, r1f); }
 
 // Stage twiddle tables, one per stage with twiddles, each laid out [r][k]:
 // entry r * NS + k = w_(R NS)^(r k) (forward sign), so that a warp's threads
@@ -309,8 +311,8 @@ constexpr int plan_m2(int n, int rl) { return plan_rest2(n, rl) / plan_m1(n, rl)
 struct TwOffsets {
   int aM1, aM2, aRL, bM2, bM1, bR1, total;
 };
-constexpr TwOffsets tw_offsets(int n, int rl) {
-  const int r1 = plan_r1(n, rl), m1 = plan_m1(n, rl), m2 = plan_m2(n, rl);
+constexpr TwOffsets tw_offsets(int n, int rl, int r1f = 0) {
+  const int r1 = plan_r1(n, rl, r1f), m1 = plan_m1(n, rl, r1f), m2 = plan_m2(n, rl, r1f);
   TwOffsets o{};
   o.aM1 = 0;
   o.aM2 = o.aM1 + (m1 > 1 ? m1 * r1 : 0);
@@ -322,11 +324,11 @@ constexpr TwOffsets tw_offsets(int n, int rl) {
   return o;
 }
 
-template <int N, int RL> struct Plan {
-  static constexpr int R1 = plan_r1(N, RL);
-  static constexpr int M1 = plan_m1(N, RL);
-  static constexpr int M2 = plan_m2(N, RL);
-  static constexpr TwOffsets TW = tw_offsets(N, RL);
+template <int N, int RL, int R1F = 0> struct Plan {
+  static constexpr int R1 = plan_r1(N, RL, R1F);
+  static constexpr int M1 = plan_m1(N, RL, R1F);
+  static constexpr int M2 = plan_m2(N, RL, R1F);
+  static constexpr TwOffsets TW = tw_offsets(N, RL, R1F);
   static_assert(R1 * M1 * M2 * RL == N, "plan");
   static_assert(M2 >= 1 && M2 <= 16, "plan depth");
   static_assert(M1 <= 16 && (16 % M1 == 0), "plan: first middle radix must divide 16");

@@ -59,9 +59,9 @@ inline uint32_t log2u(uint32_t x) {
 }
 
 // the stage twiddle tables of a length-n line FFT in the tw_offsets(n, rl) layout
-inline std::vector<HostC> stage_tables(uint32_t n, uint32_t rl) {
-  const TwOffsets o = tw_offsets((int)n, (int)rl);
-  const uint32_t r1 = plan_r1(n, rl), m1 = plan_m1(n, rl), m2 = plan_m2(n, rl);
+inline std::vector<HostC> stage_tables(uint32_t n, uint32_t rl, uint32_t r1f = 0) {
+  const TwOffsets o = tw_offsets((int)n, (int)rl, (int)r1f);
+  const uint32_t r1 = plan_r1(n, rl, r1f), m1 = plan_m1(n, rl, r1f), m2 = plan_m2(n, rl, r1f);
   std::vector<HostC> t(o.total);
   auto fill = [&](int off, uint32_t R, uint32_t NS) {
     for (uint32_t r = 0; r < R; ++r) {

@@ -71,6 +71,14 @@ int owl_plan_destroy(owl_plan* plan);
 int owl_plan_shape(const owl_plan* plan, uint32_t* N, uint32_t* W, uint32_t* H);
 /* limit of every device-side wait, in nanoseconds (default 2 s) */
 int owl_plan_set_timeout(owl_plan* plan, uint64_t ns);
+/* Split-precision form of the column pass (the reference has only FP64 kernels; this selects
+   between two implementations of its tailSquare / fftMiddleIn / fftMiddleOut step,
+   src/cl/tailsquare.cl:225-313): with enable != 0 the first forward and last inverse
+   32-point stages of every column FFT run as INT8 tensor-core GEMMs on 7 base-256 digit
+   planes of the FP64 operands (Ozaki-style), recombined exactly in FP64. Results stay bit-exact
+   while the round-off stays below 0.5 (owl_read_roe reports it). H must be 2048 (OWL_ERR_ARG
+   otherwise). Drops the plan's cached squaring graphs. */
+int owl_plan_set_split(owl_plan* plan, int enable);
 
 /* Word buffers -- Buffer<int> (src/Buffer.h:16-102), AllocTrac accounting aside. */
 int owl_buf_alloc(owl_plan* plan, int32_t** buf);

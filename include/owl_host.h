@@ -28,6 +28,7 @@ typedef struct {
   uint32_t* res_k;        /* iteration of each logged res64 */
   uint64_t* res_res64;    /* data res64 at that iteration */
   uint32_t* res_n;        /* number of checkpoints written */
+  int split;              /* 1 = split-precision column pass (owl_plan_set_split; H = 2048 shapes only) */
 } owl_run_opts;
 
 typedef struct {

@@ -5,6 +5,8 @@
 // TEST INFRASTRUCTURE ONLY. Usage:
 //   owl_emu square E W H n flags seed   (seed 0: start from 3, or 4 with LL)
 //   owl_emu modmul E W H mul3 seedA seedB
+// With OWL_EMU_SPLIT=1 in the environment and H = 2048 the column pass runs the
+// split-precision kernel (k_pass2_tc) on the emulated tensor cores.
 // Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
 #define OWL_EMU 1
 #include <cstdio>
@@ -13,6 +15,7 @@
 #include <vector>
 
 #include "owl_kernels.cuh"
+#include "owl_pass2_tc.cuh"
 #include "owl_tables.hpp"
 #include "owl_words.hpp"
 
@@ -31,6 +34,9 @@ struct EmuPlan {
   Ctl ctl{};
   std::vector<float> roe;
   int roePos = 0;
+  bool split = false;
+  std::vector<C> twHtc;
+  std::vector<uint8_t> tcB;
 };
 
 std::vector<C> toC(const std::vector<HostC>& v) {
@@ -80,6 +86,12 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   a.iscaleLo = std::ldexp(1.0, -(int)(E / p.t.N));
   a.loShift = p.t.loShift;
   a.timeoutNs = 60ull * 1000000000ull;
+  const char* sp = std::getenv("OWL_EMU_SPLIT");
+  if (sp && sp[0] == '1' && H == (uint32_t)kTcH) {
+    p.split = true;
+    p.twHtc = toC(stage_tables(H, 8, kTcR1));
+    p.tcB = tc_dft_digits();
+  }
 }
 
 template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int flags) {
@@ -93,6 +105,13 @@ template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {
   size_t sm = 2 * (size_t)p2_col_stride<H>() * sizeof(C);
   Args a = p.a;
   emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M>(a, F, Fb, Fq, -1); });
+}
+
+template <int M> void p2m_tc(EmuPlan& p, C* F, const C* Fb, C* Fq) {
+  Args a = p.a;
+  const unsigned char* tcB = p.tcB.data();
+  const C* twT = p.twHtc.data();
+  emu_launch(p.t.W / 2, kTcH / 8, kTcSmem, [=] { k_pass2_tc<kR, M>(a, tcB, twT, F, Fb, Fq, -1); });
 }
 
 template <int W> void p1w(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {
@@ -123,6 +142,13 @@ void pass1(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {
   if (p.ctl.error) { throw std::runtime_error("device wait timeout in emulation"); }
 }
 void pass2(EmuPlan& p, int mode, C* F, const C* Fb, C* Fq) {
+  if (p.split) {
+    if (mode == P2_SQUARE) p2m_tc<P2_SQUARE>(p, F, Fb, Fq);
+    else if (mode == P2_FWD) p2m_tc<P2_FWD>(p, F, Fb, Fq);
+    else p2m_tc<P2_MUL>(p, F, Fb, Fq);
+    if (p.ctl.error) { throw std::runtime_error("tensor-core wait timeout in emulation"); }
+    return;
+  }
   switch (p.t.H) {
     case 64: p2h<64>(p, mode, F, Fb, Fq); break;
     case 128: p2h<128>(p, mode, F, Fb, Fq); break;
@@ -130,6 +156,7 @@ void pass2(EmuPlan& p, int mode, C* F, const C* Fb, C* Fq) {
     case 512: p2h<512>(p, mode, F, Fb, Fq); break;
     case 640: p2h<640>(p, mode, F, Fb, Fq); break;
     case 1280: p2h<1280>(p, mode, F, Fb, Fq); break;
+    case 2048: p2h<2048>(p, mode, F, Fb, Fq); break;
     default: throw std::runtime_error("emu H");
   }
 }

@@ -20,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <stdexcept>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -50,6 +51,8 @@ struct EmuCta {
   std::vector<char> dyn;
   std::mutex m;
   std::map<int, std::vector<char>> stat;
+  std::vector<uint32_t> tmem;  // emulated tensor memory, 128 lanes x 512 columns
+  uint32_t tmemUsed = 0;
 };
 
 struct EmuThread {
@@ -84,6 +87,17 @@ template <typename T> inline T __ldcg(const T* p) { return *p; }
 inline long long __double_as_longlong(double d) { return std::bit_cast<long long>(d); }
 inline double __longlong_as_double(long long x) { return std::bit_cast<double>(x); }
 inline unsigned __float_as_uint(float f) { return std::bit_cast<unsigned>(f); }
+inline long long __double2ll_rn(double x) { return std::llrint(x); }
+inline unsigned __byte_perm(unsigned x, unsigned y, unsigned s) {
+  const uint64_t v = ((uint64_t)y << 32) | x;
+  unsigned r = 0;
+  for (int i = 0; i < 4; ++i) { r |= (unsigned)((v >> (8 * ((s >> (4 * i)) & 7))) & 0xff) << (8 * i); }
+  return r;
+}
+struct uint4 {
+  unsigned x, y, z, w;
+};
+inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return uint4{x, y, z, w}; }
 
 template <typename T> inline T emu_shfl_xor(T v, int o) {
   EmuCta* c = emu_t.cta;

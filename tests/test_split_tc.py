@@ -1,0 +1,75 @@
+"""GPU parity of the split-precision column pass (owl_plan_set_split: INT8 tensor-core GEMMs on
+base-256 digit planes for the 32-point column stages) against the GMP oracle and the plain FP64 form.
+
+Bar: bit-exact words / res64, and a round-off that stays close to the plain form's (the split form
+adds about 2^-51 relative error per GEMM output; max ROE at most 2x plain + 0.02 and below 0.35).
+"""
+import numpy as np
+import pytest
+
+from conftest import random_words, small_words
+
+pytestmark = pytest.mark.gpu
+
+# H = 2048 shapes: 256K, 2M and the 8M wavefront shape
+SPLIT_SHAPES = [(4700021, 64, 2048), (37000003, 512, 2048), (136181029, 2048, 2048)]
+
+
+@pytest.mark.parametrize("E,W,H", SPLIT_SHAPES)
+@pytest.mark.parametrize("ll", [False, True])
+def test_split_square_vs_gmp(owl, oracle, E, W, H, ll):
+    n = 20
+    with owl.Plan(E, W=W, H=H, split=True) as p:
+        start = random_words(E, E * 3 + 7)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.squareLoop(a, a, n, ll=ll)
+        got = p.readOut(a)
+    assert np.array_equal(got, oracle.gmp_square(E, start, n, ll=ll))
+
+
+@pytest.mark.parametrize("E,W,H", [SPLIT_SHAPES[0], SPLIT_SHAPES[2]])
+@pytest.mark.parametrize("mul3", [False, True])
+def test_split_modmul_vs_gmp(owl, oracle, E, W, H, mul3):
+    with owl.Plan(E, W=W, H=H, split=True) as p:
+        wa, wb = random_words(E, 15), random_words(E, 16)
+        a, b = p.alloc(), p.alloc()
+        p.writeIn(a, wa)
+        p.writeIn(b, wb)
+        p.modMul(a, b, mul3=mul3)
+        got = p.readOut(a)
+    assert np.array_equal(got, oracle.gmp_mul(E, wa, wb, mul3=mul3))
+
+
+def test_split_blocks_match_plain_and_roe(owl):
+    """2,000 graph-launched squarings at 8M from 3: identical words in both forms; ROE close."""
+    E, n = 136181029, 2000
+    out = {}
+    for split in (False, True):
+        with owl.Plan(E, W=2048, H=2048, split=split) as p:
+            a = p.alloc()
+            p.writeIn(a, small_words(E, 3))
+            p.readROE()
+            p.squareLoop(a, a, n)
+            out[split] = (p.readOut(a), float(p.readROE().max()))
+    assert np.array_equal(out[False][0], out[True][0])
+    roe_plain, roe_split = out[False][1], out[True][1]
+    assert roe_split < 0.35
+    assert roe_split <= 2 * roe_plain + 0.02, (roe_plain, roe_split)
+
+
+def test_split_prp_driver_gerbicz(owl):
+    """The C++ PRP loop (Gerbicz check every block) with the split form: same res64 checkpoints as
+    the plain form over 10,000 iterations, no check failure."""
+    E = 4700021
+    runs = [owl.prp_run(E, W=64, H=2048, block=500, log_step=1000, stop_after=10000, split=s) for s in (False, True)]
+    assert runs[1]["n_errors"] == 0 and runs[0]["n_errors"] == 0
+    assert runs[1]["k"] == runs[0]["k"] >= 10000
+    assert runs[1]["checkpoints"] == runs[0]["checkpoints"] and len(runs[0]["checkpoints"]) >= 10
+
+
+def test_split_rejects_other_heights(owl):
+    with owl.Plan(1000003, W=128, H=256) as p:
+        with pytest.raises(owl.OwlError) as e:
+            p.set_split(True)
+        assert e.value.status == -1
