@@ -92,3 +92,21 @@ def test_emulated_radix5_random_start(emu, oracle, E, W, H, n, seed):
     want = oracle.gmp_square(E, splitmix_words(E, seed), n)
     assert np.array_equal(got, want)
     assert 0 < roe < 0.1
+
+
+@pytest.mark.parametrize("mode", ["square", "modmul"])
+def test_emulated_split_precision_column_pass(emu, oracle, mode):
+    """k_pass2_tc on the emulated tensor cores (descriptor decoding, digit planes, accumulators)."""
+    E, W, H = 4700021, 64, 2048
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", OWL_EMU_SPLIT="1")
+    args = ["square", E, W, H, 2, 0, 7] if mode == "square" else ["modmul", E, W, H, 1, 11, 22]
+    r = subprocess.run([emu] + [str(a) for a in args], capture_output=True, text=True, timeout=900, env=env)
+    assert r.returncode == 0, (r.stdout[-1000:], r.stderr[-4000:])
+    lines = r.stdout.strip().split("\n")
+    got = np.array([int(x, 16) for x in lines[1].split()], dtype=np.uint32)
+    if mode == "square":
+        want = oracle.gmp_square(E, splitmix_words(E, 7), 2)
+    else:
+        want = oracle.gmp_mul(E, splitmix_words(E, 11), splitmix_words(E, 22), mul3=True)
+    assert np.array_equal(got, want)
+    assert 0 < float(lines[0].split()[1]) < 0.1
