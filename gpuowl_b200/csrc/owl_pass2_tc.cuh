@@ -100,9 +100,9 @@ __device__ __forceinline__ void tc_put_digits(unsigned char* sA, int row, int hh
 // issues the 56 MMAs of one N half: accumulator d (TMEM columns 32 d ..) gets sum_{i+j=d} A_i B_j^T
 __device__ __forceinline__ void tc_issue(uint32_t aBase, uint32_t bBase, uint32_t taddr, int half) {
   constexpr uint32_t idesc = tc::idesc_s8(kTcRows, kTcNHalf);
-#pragma unroll 1
+#pragma unroll
   for (int d = 0; d < kTcSlices; ++d) {
-#pragma unroll 1
+#pragma unroll
     for (int i = 0; i <= d; ++i) {
       const int j = d - i;
 #pragma unroll
@@ -152,20 +152,39 @@ __device__ __forceinline__ bool tc_dft32(const Args& a, unsigned char* sA, int* 
     ok &= tc::mbar_wait(sBar, phase & 1u, a.timeoutNs);
     ++phase;
     tc::fence_after();
-    double acc[16];
+    // D_d < (d + 1) 2^20, so D0 256 + D1, D2 256 + D3 and D4 256 + D5 are exact in INT32; the
+    // rest of Horner's rule runs in FP64 (exact up to the last two steps, one rounding each)
 #pragma unroll
-    for (int i = 0; i < 16; ++i) { acc[i] = 0.0; }
-#pragma unroll
-    for (int d = 0; d < kTcSlices; ++d) {
-      uint32_t r[16];
-      tc::tmem_ld16(taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(d * kTcNHalf + cs), r);
+    for (int g = 0; g < 2; ++g) {
+      const uint32_t tb = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(cs + 8 * g);
+      uint32_t ra[8], rb[8];
+      int32_t p01[8], p23[8], p45[8];
+      tc::tmem_ld8(tb + 0 * kTcNHalf, ra);
+      tc::tmem_ld8(tb + 1 * kTcNHalf, rb);
       tc::tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) { acc[i] = fma(acc[i], 256.0, (double)(int32_t)r[i]); }
-    }
+      for (int i = 0; i < 8; ++i) { p01[i] = (int32_t)ra[i] * 256 + (int32_t)rb[i]; }
+      tc::tmem_ld8(tb + 2 * kTcNHalf, ra);
+      tc::tmem_ld8(tb + 3 * kTcNHalf, rb);
+      tc::tmem_wait_ld();
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      y[half * 8 + k] = mk(acc[2 * k] * post, (INV ? -post : post) * acc[2 * k + 1]);
+      for (int i = 0; i < 8; ++i) { p23[i] = (int32_t)ra[i] * 256 + (int32_t)rb[i]; }
+      tc::tmem_ld8(tb + 4 * kTcNHalf, ra);
+      tc::tmem_ld8(tb + 5 * kTcNHalf, rb);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 8; ++i) { p45[i] = (int32_t)ra[i] * 256 + (int32_t)rb[i]; }
+      tc::tmem_ld8(tb + 6 * kTcNHalf, ra);
+      tc::tmem_wait_ld();
+      double v[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        double acc = fma(tc::i32_to_f64(p01[i]), 65536.0, tc::i32_to_f64(p23[i]));
+        acc = fma(acc, 65536.0, tc::i32_to_f64(p45[i]));
+        v[i] = fma(acc, 256.0, tc::i32_to_f64((int32_t)ra[i])) * post;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { y[half * 8 + 4 * g + k] = mk(v[2 * k], INV ? -v[2 * k + 1] : v[2 * k + 1]); }
     }
     tc::fence_before();
     __syncthreads();  // all accumulator reads done before the next batch overwrites them

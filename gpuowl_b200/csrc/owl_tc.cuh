@@ -37,6 +37,10 @@ __host__ __device__ constexpr uint64_t smem_desc(uint32_t saddr, uint32_t lbo, u
 }
 
 __device__ __forceinline__ double exp2i(int k) { return __longlong_as_double((long long)(1023 + k) << 52); }
+// exact int32 -> double without the conversion unit: 2^52 + 2^31 + v built from its bits, minus 2^52 + 2^31
+__device__ __forceinline__ double i32_to_f64(int32_t v) {
+  return __hiloint2double(0x43300000, (int)((uint32_t)v ^ 0x80000000u)) - 4503601774854144.0;
+}
 
 #ifndef OWL_EMU
 
@@ -104,6 +108,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr)
       : "memory");
+}
+// warp-collective: 32 lanes x 8 consecutive 32-bit columns
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr)
+               : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -180,6 +191,13 @@ inline void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   const uint32_t lane0 = taddr >> 16, col0 = taddr & 0xFFFFu;
   if (lane0 != 32 * (w % 4) || col0 + 16 > 512) { throw std::runtime_error("emu: tensor-memory read out of range"); }
   for (int i = 0; i < 16; ++i) { r[i] = c->tmem[(size_t)(lane0 + lane) * 512 + col0 + i]; }
+}
+inline void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  EmuCta* c = emu_t.cta;
+  const uint32_t w = emu_t.tid.x / 32, lane = emu_t.tid.x % 32;
+  const uint32_t lane0 = taddr >> 16, col0 = taddr & 0xFFFFu;
+  if (lane0 != 32 * (w % 4) || col0 + 8 > 512) { throw std::runtime_error("emu: tensor-memory read out of range"); }
+  for (int i = 0; i < 8; ++i) { r[i] = c->tmem[(size_t)(lane0 + lane) * 512 + col0 + i]; }
 }
 inline void tmem_wait_ld() {}
 

@@ -88,6 +88,9 @@ inline long long __double_as_longlong(double d) { return std::bit_cast<long long
 inline double __longlong_as_double(long long x) { return std::bit_cast<double>(x); }
 inline unsigned __float_as_uint(float f) { return std::bit_cast<unsigned>(f); }
 inline long long __double2ll_rn(double x) { return std::llrint(x); }
+inline double __hiloint2double(int hi, int lo) {
+  return std::bit_cast<double>(((uint64_t)(uint32_t)hi << 32) | (uint32_t)lo);
+}
 inline unsigned __byte_perm(unsigned x, unsigned y, unsigned s) {
   const uint64_t v = ((uint64_t)y << 32) | x;
   unsigned r = 0;
