@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""bench.py -- ms per PRP-3 iteration at the 8M FFT on B200 (libowl, plain FP64 form).
+"""bench.py -- ms per PRP-3 iteration at the 8M FFT on B200 (libowl): the plain FP64 form
+(the headline value) and the split-precision tensor-core form ("split_tc"), both bit-exact.
 
 Workload (one "step" = one Gerbicz block of the reference's PRP loop,
 src/Gpu.cpp:1461-1483): modMul(check, data) then 1,000 squarings of data,
@@ -44,6 +45,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--block", type=int, default=BLOCK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tensor-core) form")
     ap.add_argument("--workload", default="prp8m", choices=["prp8m", "batch64"],
                     help="prp8m: the headline line; batch64: 64 uneven exponents in one graph per block")
     return ap.parse_args()
@@ -131,6 +133,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_bf16():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
 def profiled_traffic():
     """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "traffic_8m.json")
@@ -211,6 +221,7 @@ def run_reference(args, rank, world):
 
 
 def run_ours(args, rank, world, local):
+    import numpy as np
     import torch
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
@@ -228,71 +239,106 @@ def run_ours(args, rank, world, local):
             dist.barrier()
 
     B = args.block
-    plan = owl.Plan(E_8M, device=local, W=W_8M, H=H_8M)
-    stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", local))
-    data, check, aux = plan.alloc(), plan.alloc(), plan.alloc()
-    one = [1] + [0] * (plan.nwords - 1)
-    three = [3] + [0] * (plan.nwords - 1)
-    plan.writeIn(data, three)
-    plan.writeIn(check, one)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     golden = load_golden("prp_8m")
-    res = []
 
-    def step():
-        plan.modMul(check, data)
-        return plan.profile_square(data, B)
+    def measure(split, steps, warmup, with_e2e):
+        """Timed PRP blocks of one form: CUDA-event step times, per-kernel device times from the
+        launch stamps, res64 per block against the golden table, a final Gerbicz check and
+        (with_e2e) the host-buffer end-to-end loop through the public API."""
+        plan = owl.Plan(E_8M, device=local, W=W_8M, H=H_8M, split=split)
+        stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", local))
+        data, check, aux = plan.alloc(), plan.alloc(), plan.alloc()
+        plan.writeIn(data, [3] + [0] * (plan.nwords - 1))
+        plan.writeIn(check, [1] + [0] * (plan.nwords - 1))
+        res = []
 
-    for _ in range(args.warmup):
-        step()
-        res.append("%016x" % plan.bufResidue(data))
-    plan.readROE()
+        def step():
+            plan.modMul(check, data)
+            return plan.profile_square(data, B)
 
-    step_ms, prof = [], {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            p = step()
-            e1.record(stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            for k, (ms, n) in p.items():
-                prof[k][0] += ms
-                prof[k][1] += n
+        for _ in range(warmup):
+            step()
             res.append("%016x" % plan.bufResidue(data))
-    torch.cuda.synchronize()
-    barrier()
-    total_ms = sum(step_ms)
-    roe = plan.readROE()
-
-    # Gerbicz check of the final state (reference doCheck, src/Gpu.cpp:767-771)
-    plan.squareLoop(aux, check, B, mul3=True)
-    plan.modMul(check, data)
-    gerbicz_ok = plan.isEqual(check, aux)
-
-    # e2e through the public API with host buffers: writeIn -> block -> readOut (+res64)
-    words = plan.readOut(data)
-    e2e_ms = []
-    barrier()
-    for _ in range(max(2, args.steps // 2)):
+        plan.readROE()
+        step_ms, prof = [], {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
+        barrier()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        plan.writeIn(data, words)
+        with ClockSampler(local) as clocks:
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                pr = step()
+                e1.record(stream)
+                e1.synchronize()
+                step_ms.append(e0.elapsed_time(e1))
+                for k, (ms, n) in pr.items():
+                    prof[k][0] += ms
+                    prof[k][1] += n
+                res.append("%016x" % plan.bufResidue(data))
+        torch.cuda.synchronize()
+        barrier()
+        roe = plan.readROE()
+        # Gerbicz check of the final state (reference doCheck, src/Gpu.cpp:767-771)
+        plan.squareLoop(aux, check, B, mul3=True)
         plan.modMul(check, data)
-        plan.squareLoop(data, data, B)
-        words = plan.readOut(data)
-        e2e_ms.append(1e3 * (time.perf_counter() - t0))
-    barrier()
+        gerbicz_ok = plan.isEqual(check, aux)
+        e2e_ms = []
+        if with_e2e:
+            # e2e through the public API with host buffers: writeIn -> block -> readOut (+res64)
+            words = plan.readOut(data)
+            barrier()
+            for _ in range(max(2, steps // 2)):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                plan.writeIn(data, words)
+                plan.modMul(check, data)
+                plan.squareLoop(data, data, B)
+                words = plan.readOut(data)
+                e2e_ms.append(1e3 * (time.perf_counter() - t0))
+            barrier()
+        plan.close()
+        n = min(len(res), len(golden["res64"])) if golden else 0
+        return {"total_ms": sum(step_ms), "prof": prof, "roe": float(roe.max()) if roe.size else None,
+                "gerbicz_ok": bool(gerbicz_ok), "res_match": (res[:n] == golden["res64"][:n]) if golden else None,
+                "res_checked": n, "clocks": clocks.summary(), "e2e_ms": e2e_ms}
 
+    plain = measure(False, args.steps, args.warmup, True)
+    split = measure(True, args.steps, args.warmup, False) if not args.no_split else None
+    total_ms, prof, roe = plain["total_ms"], plain["prof"], plain["roe"]
+    e2e_ms = plain["e2e_ms"]
     total_ms, e2e_step, value = replica_summary(dist, total_ms, sum(e2e_ms) / len(e2e_ms), args.steps, B, world,
                                                 device="cuda")
-    n = min(len(res), len(golden["res64"])) if golden else 0
-    res_match = (res[:n] == golden["res64"][:n]) if golden else None
+    split_line = None
+    if split is not None:
+        s_total, _, s_value = replica_summary(dist, split["total_ms"], 0.0, args.steps, B, world, device="cuda")
+        sp = split["prof"]
+        tc_ms = sp["pass2"][0] / max(sp["pass2"][1], 1)
+        # INT8 work of one k_pass2_tc launch: W/2 CTAs x 4 GEMM halves x 56 MMAs of 128 x 32 x 32
+        tc_ops = 2.0 * (W_8M // 2) * 4 * 56 * 128 * 32 * 32
+        bf16 = measured_bf16()
+        split_line = {
+            "form": "split-precision: 32-point column stages as INT8 tcgen05 GEMMs on 7 base-256 digit planes",
+            "ms_per_iter": round(s_value, 5), "ms_per_step": round(s_total / args.steps, 4),
+            "kernel_ms": {k: round(v[0] / max(v[1], 1), 5) for k, v in sp.items()},
+            "max_roe": round(split["roe"], 5) if split["roe"] is not None else None,
+            "max_roe_plain": round(roe, 5) if roe is not None else None,
+            "res64_match_golden": split["res_match"], "res64_checked": split["res_checked"],
+            "gerbicz_ok": split["gerbicz_ok"],
+            "tensor_roofline": {"bound": "tensor", "kernel": "k_pass2_tc",
+                                "achieved": round(tc_ops / (tc_ms * 1e-3) / 1e12, 2),
+                                "peak": round(2 * bf16[0], 1), "unit": "TOP/s (int8)",
+                                "frac": round(tc_ops / (tc_ms * 1e-3) / 1e12 / (2 * bf16[0]), 4),
+                                "peak_kind": "2 x %s bf16 dense (int8 dense rate is twice bf16's)" % bf16[1],
+                                "int8_ops_per_launch": tc_ops},
+            "gpu_launches": (5 + 2 * B + 1) * args.steps,
+            "clocks": split["clocks"],
+            "vs_plain": round(s_value / value, 3),
+        }
+    res_match, n, gerbicz_ok, clocks = plain["res_match"], plain["res_checked"], plain["gerbicz_ok"], plain["clocks"]
+    roe = np.array([roe]) if roe is not None else np.array([])
 
     # roofline of the dominant kernel: algorithmic bytes per launch = read + write of the
     # 8N-byte state = 16 N bytes, over its average launch time in the timed region
@@ -331,6 +377,7 @@ def run_ours(args, rank, world, local):
                    "parallelism": "replicas x%d" % world},
         "res64_match_golden": res_match, "res64_checked": n, "gerbicz_ok": bool(gerbicz_ok),
         "max_roe": round(float(roe.max()), 5) if roe.size else None,
+        "split_tc": split_line,
         "kernel_ms": {k: round(v[0] / max(v[1], 1), 5) for k, v in prof.items()},
         "roofline": {"bound": "hbm", "kernel": "k_pass2" if dom == "pass2" else "k_pass1",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -340,7 +387,7 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": round(e2e_step / B, 5), "unit": "ms/iter",
                 "h2d_bytes_per_step": 4 * N_8M, "d2h_bytes_per_step": 4 * N_8M + 8},
         "gpu_launches": launches_per_step * args.steps,
-        "clocks": clocks.summary(),
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
