@@ -19,6 +19,7 @@
 #include "owl.h"
 #include "owl_kernels.cuh"
 #include "owl_pass2_tc.cuh"
+#include "owl_pack.cuh"
 #include "owl_tables.hpp"
 #include "owl_words.hpp"
 
@@ -117,6 +118,11 @@ struct owl_plan {
   bool split = false;
   const unsigned char* tcB = nullptr;
   const C* twHtc = nullptr;
+  // device-side expand / compact: word staging (nWords + 1, zero padded), block carries, status
+  uint32_t* dwords = nullptr;
+  uint32_t* packBlk = nullptr;
+  owl::PackCtl* packCtl = nullptr;
+  uint32_t nw = 0, packBlocks = 0;
 };
 
 namespace {
@@ -456,7 +462,9 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
 
   // scratch: carry shuttle, flags, control word, ROE slots, small outputs
   const uint32_t G = H / kR;
-  size_t sbytes = 256 * 11 + (size_t)G * W * sizeof(long long) + G * sizeof(uint32_t) + sizeof(owl::Ctl) +
+  const uint32_t nw = owl::n_words(E), packBlocks = (N + owl::kPackDigits - 1) / owl::kPackDigits;
+  size_t sbytes = 256 * 14 + (size_t)G * W * sizeof(long long) + G * sizeof(uint32_t) + sizeof(owl::Ctl) +
+                  (size_t)(nw + 2) * sizeof(uint32_t) + packBlocks * sizeof(uint32_t) + sizeof(owl::PackCtl) +
                   2 * owl::kPendingCap * sizeof(long long) + 2 * kTsCap * sizeof(unsigned long long) +
                   kRoeCap * sizeof(float) + 64 * sizeof(int32_t) + sizeof(unsigned long long) + sizeof(int);
   ck(cudaMalloc(&p->scratch, sbytes), "cudaMalloc(scratch)");
@@ -472,6 +480,11 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   p->small = carve<int32_t>(cur, 64);
   p->sum = carve<unsigned long long>(cur, 1);
   p->eq = carve<int>(cur, 1);
+  p->dwords = carve<uint32_t>(cur, nw + 2);
+  p->packBlk = carve<uint32_t>(cur, packBlocks);
+  p->packCtl = carve<owl::PackCtl>(cur, 1);
+  p->nw = nw;
+  p->packBlocks = packBlocks;
 
   p->args.E = E;
   p->args.N = N;
@@ -500,20 +513,45 @@ void plan_destroy(owl_plan* p) {
   delete p;
 }
 
-void checked_download(owl_plan* p, const int32_t* buf, std::vector<int32_t>& host) {
-  host.resize(p->N);
+// compact words (host) -> balanced digits in buf, on the device (reference expandBits)
+void expand_on_device(owl_plan* p, int32_t* buf, const uint32_t* words) {
+  ck(cudaMemcpyAsync(p->dwords, words, (size_t)p->nw * sizeof(uint32_t), cudaMemcpyHostToDevice, p->stream),
+     "upload words");
+  owl::k_pack_summary<true><<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(p->dwords, nullptr, p->nw, p->E,
+                                                                                 p->N, p->packBlk);
+  owl::k_pack_chain<<<1, 32, 0, p->stream>>>(p->packBlk, p->packBlocks, p->packCtl);
+  owl::k_expand_digits<<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(p->dwords, p->nw, p->E, p->N, p->packBlk,
+                                                                             p->packCtl, buf);
+  ck(cudaGetLastError(), "expand launch");
+  sync_and_check(p);
+}
+
+// balanced digits in buf -> compact words (host), on the device (reference compactBits), read back
+// with a device checksum compared on the host (reference readChecked, src/Gpu.cpp:677-705)
+void compact_on_device(owl_plan* p, const int32_t* buf, uint32_t* words) {
   for (int attempt = 0; attempt < 3; ++attempt) {
+    ck(cudaMemsetAsync(p->dwords, 0, (size_t)(p->nw + 2) * sizeof(uint32_t), p->stream), "memset words");
+    owl::k_pack_summary<false><<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(nullptr, buf, p->nw, p->E, p->N,
+                                                                                    p->packBlk);
+    owl::k_pack_chain<<<1, 32, 0, p->stream>>>(p->packBlk, p->packBlocks, p->packCtl);
+    owl::k_compact_words<<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(buf, p->nw, p->E, p->N, p->packBlk,
+                                                                               p->packCtl, p->dwords);
+    owl::k_compact_finish<<<1, 32, 0, p->stream>>>(p->packCtl, p->nw, p->dwords);
     ck(cudaMemsetAsync(p->sum, 0, sizeof(unsigned long long), p->stream), "memset sum");
-    owl::k_sum64<<<296, 256, 0, p->stream>>>(reinterpret_cast<const unsigned long long*>(buf), p->N / 2, p->sum);
-    ck(cudaGetLastError(), "sum64 launch");
+    owl::k_sum64<<<296, 256, 0, p->stream>>>(reinterpret_cast<const unsigned long long*>(p->dwords), (p->nw + 1) / 2,
+                                             p->sum);
+    ck(cudaGetLastError(), "compact launch");
     unsigned long long gpuSum = 0;
+    owl::PackCtl ctl{};
     ck(cudaMemcpyAsync(&gpuSum, p->sum, sizeof(gpuSum), cudaMemcpyDeviceToHost, p->stream), "read sum");
-    ck(cudaMemcpyAsync(host.data(), buf, (size_t)p->N * sizeof(int32_t), cudaMemcpyDeviceToHost, p->stream),
+    ck(cudaMemcpyAsync(&ctl, p->packCtl, sizeof(ctl), cudaMemcpyDeviceToHost, p->stream), "read status");
+    ck(cudaMemcpyAsync(words, p->dwords, (size_t)p->nw * sizeof(uint32_t), cudaMemcpyDeviceToHost, p->stream),
        "read words");
     sync_and_check(p);
+    if (ctl.error) { fail(OWL_ERR_READ, "digit out of range"); }
     unsigned long long hostSum = 0;
-    for (uint32_t i = 0; i + 1 < p->N; i += 2) {
-      hostSum += (uint64_t)(uint32_t)host[i] | ((uint64_t)(uint32_t)host[i + 1] << 32);
+    for (uint32_t i = 0; i < p->nw; i += 2) {
+      hostSum += (uint64_t)words[i] | ((i + 1 < p->nw ? (uint64_t)words[i + 1] : 0) << 32);
     }
     if (hostSum == gpuSum) { return; }
   }
@@ -706,12 +744,9 @@ int owl_write_words(owl_plan* plan, int32_t* buf, const uint32_t* words) {
     check_plan(plan);
     check_buf(plan, buf);
     if (!words) { fail(OWL_ERR_ARG, "null words"); }
-    std::vector<int32_t> d(plan->N);
-    if (!owl::expand_bits(words, plan->N, plan->E, d.data())) { fail(OWL_ERR_ARG, "expandBits failed"); }
+    if (plan->E % 32 == 0) { fail(OWL_ERR_ARG, "expandBits failed"); }
     DeviceGuard dg(plan->device);
-    ck(cudaMemcpyAsync(buf, d.data(), (size_t)plan->N * sizeof(int32_t), cudaMemcpyHostToDevice, plan->stream),
-       "upload");
-    ck(cudaStreamSynchronize(plan->stream), "sync");
+    expand_on_device(plan, buf, words);
   });
 }
 
@@ -721,9 +756,7 @@ int owl_read_words(owl_plan* plan, const int32_t* buf, uint32_t* words) {
     check_buf(plan, buf);
     if (!words) { fail(OWL_ERR_ARG, "null words"); }
     DeviceGuard dg(plan->device);
-    std::vector<int32_t> d;
-    checked_download(plan, buf, d);
-    if (!owl::compact_bits(d.data(), plan->N, plan->E, words)) { fail(OWL_ERR_READ, "digit out of range"); }
+    compact_on_device(plan, buf, words);
   });
 }
 
@@ -787,10 +820,8 @@ int owl_res64(owl_plan* plan, const int32_t* buf, uint64_t* res64) {
     bool decided = false;
     uint64_t r = owl::residue_from_wrap(w, plan->N, plan->E, &decided);
     if (!decided) {
-      std::vector<int32_t> d;
-      checked_download(plan, buf, d);
       std::vector<uint32_t> words(owl::n_words(plan->E));
-      if (!owl::compact_bits(d.data(), plan->N, plan->E, words.data())) { fail(OWL_ERR_READ, "digit out of range"); }
+      compact_on_device(plan, buf, words.data());
       r = (uint64_t)words[0] | ((words.size() > 1 ? (uint64_t)words[1] : 0) << 32);
     }
     *res64 = r;

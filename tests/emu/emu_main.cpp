@@ -5,10 +5,12 @@
 // TEST INFRASTRUCTURE ONLY. Usage:
 //   owl_emu square E W H n flags seed   (seed 0: start from 3, or 4 with LL)
 //   owl_emu modmul E W H mul3 seedA seedB
+//   owl_emu pack E N pattern            (device expand / compact vs owl_words.hpp; prints "pack ok")
 // With OWL_EMU_SPLIT=1 in the environment and H = 2048 the column pass runs the
 // split-precision kernel (k_pass2_tc) on the emulated tensor cores.
 // Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
 #define OWL_EMU 1
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -16,6 +18,7 @@
 
 #include "owl_kernels.cuh"
 #include "owl_pass2_tc.cuh"
+#include "owl_pack.cuh"
 #include "owl_tables.hpp"
 #include "owl_words.hpp"
 
@@ -207,10 +210,76 @@ float max_roe(const EmuPlan& p) {
 
 }  // namespace
 
+// pattern 0: 3, 1: 2^E - 1, 2: every raw digit 2^(len-1) - 1 (a carry that propagates through all
+// digits), 3: zero, 4: 2^E - 2, other: random words from that seed
+std::vector<uint32_t> pack_words(uint32_t E, uint32_t N, uint64_t pattern) {
+  const uint32_t nw = n_words(E);
+  std::vector<uint32_t> w(nw, 0);
+  auto mask_top = [&] {
+    if (E % 32) { w.back() &= (1u << (E % 32)) - 1; }
+  };
+  if (pattern == 0) {
+    w[0] = 3;
+  } else if (pattern == 1 || pattern == 4) {
+    for (auto& x : w) { x = 0xffffffffu; }
+    mask_top();
+    if (pattern == 4) { w[0] -= 1; }
+  } else if (pattern == 2) {
+    uint64_t bit = 0;
+    for (uint32_t k = 0; k < N; ++k) {
+      const uint32_t len = word_bits(N, E, k);
+      const uint64_t v = (1ull << (len - 1)) - 1;
+      for (uint32_t b = 0; b < len; ++b, ++bit) {
+        if ((v >> b) & 1) { w[bit / 32] |= 1u << (bit % 32); }
+      }
+    }
+  } else if (pattern != 3) {
+    w = start_words(E, pattern, 3);
+  }
+  return w;
+}
+
+int pack_test(uint32_t E, uint32_t N, uint64_t pattern) {
+  const uint32_t nw = n_words(E), nb = (N + kPackDigits - 1) / kPackDigits;
+  std::vector<uint32_t> words = pack_words(E, N, pattern), blk(nb), dwords(nw + 2, 0), want(nw);
+  std::vector<int32_t> host(N), dev(N);
+  PackCtl ctl{};
+  if (!expand_bits(words.data(), N, E, host.data())) { return 3; }
+  const uint32_t* pw = words.data();
+  uint32_t* pb = blk.data();
+  int32_t* pd = dev.data();
+  PackCtl* pc = &ctl;
+  emu_launch(nb, kPackThreads, 0, [=] { k_pack_summary<true>(pw, nullptr, nw, E, N, pb); });
+  emu_launch(1, 32, 0, [=] { k_pack_chain(pb, nb, pc); });
+  emu_launch(nb, kPackThreads, 0, [=] { k_expand_digits(pw, nw, E, N, pb, pc, pd); });
+  if (dev != host) {
+    std::printf("error expand differs\n");
+    return 5;
+  }
+  // compact the digits back and compare with the host compact
+  if (!compact_bits(host.data(), N, E, want.data())) { return 3; }
+  const int32_t* ph = host.data();
+  uint32_t* po = dwords.data();
+  emu_launch(nb, kPackThreads, 0, [=] { k_pack_summary<false>(nullptr, ph, nw, E, N, pb); });
+  emu_launch(1, 32, 0, [=] { k_pack_chain(pb, nb, pc); });
+  emu_launch(nb, kPackThreads, 0, [=] { k_compact_words(ph, nw, E, N, pb, pc, po); });
+  emu_launch(1, 32, 0, [=] { k_compact_finish(pc, nw, po); });
+  if (ctl.error || !std::equal(want.begin(), want.end(), dwords.begin())) {
+    std::printf("error compact differs\n");
+    return 6;
+  }
+  std::printf("pack ok\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) { return 2; }
   std::string mode = argv[1];
   try {
+    if (mode == "pack" && argc == 5) {
+      return pack_test(std::strtoul(argv[2], nullptr, 10), std::strtoul(argv[3], nullptr, 10),
+                       std::strtoull(argv[4], nullptr, 10));
+    }
     if (mode == "square" && argc == 8) {
       uint32_t E = std::strtoul(argv[2], nullptr, 10), W = std::strtoul(argv[3], nullptr, 10),
                H = std::strtoul(argv[4], nullptr, 10), n = std::strtoul(argv[5], nullptr, 10),

@@ -260,3 +260,44 @@ def test_batch_of_uneven_exponents_matches_gmp(owl, oracle):
     finally:
         for p in plans:
             p.close()
+
+
+def _pattern_words(E, N, pattern):
+    """0: 3, 1: 2^E - 1, 2: every raw digit 2^(bits-1) - 1 (one carry runs through all digits),
+    3: zero, 4: 2^E - 2, else random."""
+    nw = (E - 1) // 32 + 1
+    if pattern == 0:
+        return small_words(E, 3)
+    if pattern in (1, 4):
+        w = np.full(nw, 0xffffffff, dtype=np.uint32)
+        w[-1] &= (1 << (E % 32)) - 1
+        if pattern == 4:
+            w[0] -= 1
+        return w
+    if pattern == 2:
+        x, off = 0, 0
+        for k in range(N):
+            nxt = -(-(k + 1) * E // N)
+            ln = nxt - off
+            x |= ((1 << (ln - 1)) - 1) << off
+            off = nxt
+        return np.frombuffer(x.to_bytes(4 * nw, "little"), dtype=np.uint32).copy()
+    if pattern == 3:
+        return np.zeros(nw, dtype=np.uint32)
+    return random_words(E, pattern)
+
+
+@pytest.mark.parametrize("E,W,H", [SHAPES[0], SHAPES[5], SHAPES[10], SHAPES_WIDE[0]])
+@pytest.mark.parametrize("pattern", [0, 1, 2, 3, 4, 77])
+def test_device_expand_compact_match_host(owl, oracle, E, W, H, pattern):
+    """owl_write_words / owl_read_words convert on the device; the digits and words must equal the
+    host restatement of the reference's expandBits / compactBits bit for bit."""
+    with owl.Plan(E, W=W, H=H) as p:
+        if pattern == 2 and p.N > (1 << 18):
+            pytest.skip("pattern built digit by digit in Python; small N only")
+        words = _pattern_words(E, p.N, pattern)
+        a = p.alloc()
+        p.writeIn(a, words)
+        digits = p.read_digits(a)
+        assert np.array_equal(digits, oracle.expand(E, p.N, words))
+        assert np.array_equal(p.readOut(a), oracle.compact(E, p.N, digits))
