@@ -34,6 +34,7 @@ SEED = 20261203
 E_8M = 136181029      # oracle_seeded_prime(SEED + 2, 136M, 139M)
 W_8M, H_8M = 2048, 2048
 N_8M = 2 * W_8M * H_8M
+NW_8M = (E_8M - 1) // 32 + 1
 BLOCK = 1000
 
 
@@ -385,7 +386,9 @@ def run_ours(args, rank, world, local):
                      "traffic": traffic, "alg_bytes_per_launch": alg_bytes},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_step / B, 5), "unit": "ms/iter",
-                "h2d_bytes_per_step": 4 * N_8M, "d2h_bytes_per_step": 4 * N_8M + 8},
+                "h2d_bytes_per_step": 4 * NW_8M, "d2h_bytes_per_step": 4 * NW_8M + 16,
+                "step": "owl_write_words (E-bit words, expanded on the device) + modMul + %d squarings + "
+                        "owl_read_words (compacted on the device, checksummed)" % B},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
     }
