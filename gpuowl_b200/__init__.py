@@ -46,13 +46,14 @@ class RunOpts(ctypes.Structure):
                 ("H", ctypes.c_uint32), ("save_dir", ctypes.c_char_p), ("inject_fault_k", ctypes.c_uint32),
                 ("verbose", ctypes.c_int), ("res_cap", ctypes.c_uint32), ("res_k", ctypes.POINTER(ctypes.c_uint32)),
                 ("res_res64", ctypes.POINTER(ctypes.c_uint64)), ("res_n", ctypes.POINTER(ctypes.c_uint32)),
-                ("split", ctypes.c_int)]
+                ("split", ctypes.c_int), ("proof_power", ctypes.c_uint32)]
 
 
 class RunResult(ctypes.Structure):
     """owl_run_result (include/owl_host.h)."""
     _fields_ = [("is_prime", ctypes.c_int), ("finished", ctypes.c_int), ("k", ctypes.c_uint32),
-                ("res64", ctypes.c_uint64), ("n_errors", ctypes.c_uint32), ("res2048", ctypes.c_char * 513)]
+                ("res64", ctypes.c_uint64), ("n_errors", ctypes.c_uint32), ("res2048", ctypes.c_char * 513),
+                ("proof_power", ctypes.c_uint32), ("proof_file", ctypes.c_char * 1024)]
 
 
 _SIGS = {
@@ -95,6 +96,11 @@ _SIGS = {
     "owl_ll_save": ([ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, _U32P, ctypes.c_double], ctypes.c_int),
     "owl_ll_load": ([ctypes.c_char_p, ctypes.c_uint32, _U32P, _U32P, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "owl_crc32": ([ctypes.c_void_p, ctypes.c_size_t], ctypes.c_uint32),
+    "owl_sha3_256": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint8)], None),
+    "owl_proof_points": ([ctypes.c_uint32, ctypes.c_uint32, _U32P, ctypes.c_uint32, _U32P], ctypes.c_int),
+    "owl_proof_verify": ([ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+                         ctypes.c_int),
+    "owl_exp_mul": ([_P, _P, ctypes.c_uint64, _P], ctypes.c_int),
     "owl_batch_create": ([ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(_P), ctypes.POINTER(_P)], ctypes.c_int),
     "owl_batch_square": ([_P, ctypes.POINTER(_P), ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int),
     "owl_batch_sync": ([_P], ctypes.c_int),
@@ -246,6 +252,10 @@ class Plan:
         flags = (SQ_MUL3 if mul3 else 0) | (SQ_LL if ll else 0)
         _check(self.lib.owl_square(self.h, out, inp, int(n), flags))
 
+    def expMul(self, a, h, b):
+        """a := a^h * b (reference Gpu::expMul; a and b different buffers)."""
+        _check(self.lib.owl_exp_mul(self.h, a, int(h), b))
+
     def modMul(self, io_a, in_b, mul3=False):
         _check(self.lib.owl_modmul(self.h, io_a, in_b, 1 if mul3 else 0))
 
@@ -294,26 +304,53 @@ class Plan:
 # ---- host drivers (include/owl_host.h) ----
 
 def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, W, H, inject_fault_k, verbose,
-         n_savefiles=4, cap=4096, split=False):
+         n_savefiles=4, cap=4096, split=False, proof_power=0):
     lib = load()
     ks = (ctypes.c_uint32 * cap)()
     rs = (ctypes.c_uint64 * cap)()
     n = ctypes.c_uint32(0)
     o = RunOpts(block, log_step, check_step, stop_after, n_savefiles, W, H,
                 save_dir.encode() if save_dir else None, inject_fault_k, 1 if verbose else 0, cap,
-                ks, rs, ctypes.pointer(n), 1 if split else 0)
+                ks, rs, ctypes.pointer(n), 1 if split else 0, int(proof_power))
     r = RunResult()
     _check(getattr(lib, fn_name)(device, E, ctypes.byref(o), ctypes.byref(r)))
     return {"is_prime": bool(r.is_prime), "finished": bool(r.finished), "k": r.k, "res64": r.res64,
             "n_errors": r.n_errors, "res2048": r.res2048.decode(),
+            "proof_power": r.proof_power, "proof_file": r.proof_file.decode() or None,
             "checkpoints": [(ks[i], rs[i]) for i in range(n.value)]}
 
 
 def prp_run(E, device=0, block=1000, log_step=20000, check_step=0, stop_after=0, save_dir=None, W=0, H=0,
-            inject_fault_k=0, verbose=False, split=False):
-    """PRP-3 test (the reference's Gpu::isPrimePRP) through owl_prp_run."""
+            inject_fault_k=0, verbose=False, split=False, proof_power=0):
+    """PRP-3 test (the reference's Gpu::isPrimePRP) through owl_prp_run; with proof_power > 0 the
+    proof residues go to save_dir/<E>/proof/ and the verified proof to save_dir/proof/<E>-<p>.proof."""
     return _run("owl_prp_run", E, device, block, log_step, check_step, stop_after, save_dir, W, H,
-                inject_fault_k, verbose, split=split)
+                inject_fault_k, verbose, split=split, proof_power=proof_power)
+
+
+def sha3_256(data):
+    """SHA3-256 digest (bytes) of `data` with the library's proof hash."""
+    b = bytes(data)
+    out = (ctypes.c_uint8 * 32)()
+    load().owl_sha3_256(b, len(b), out)
+    return bytes(out)
+
+
+def proof_points(E, power):
+    """Iterations whose residues a power-`power` proof needs (increasing, the last = E)."""
+    lib = load()
+    n = ctypes.c_uint32(0)
+    _check(lib.owl_proof_points(E, power, None, 0, ctypes.byref(n)))
+    arr = (ctypes.c_uint32 * n.value)()
+    _check(lib.owl_proof_points(E, power, arr, n.value, ctypes.byref(n)))
+    return list(arr)
+
+
+def proof_verify(path, device=0):
+    """(valid, is_prime) of a proof file (reference Proof::verify)."""
+    v, p = ctypes.c_int(0), ctypes.c_int(0)
+    _check(load().owl_proof_verify(device, str(path).encode(), ctypes.byref(v), ctypes.byref(p)))
+    return bool(v.value), bool(p.value)
 
 
 def ll_run(E, device=0, log_step=10000, stop_after=0, save_dir=None, W=0, H=0, verbose=False, split=False):

@@ -788,6 +788,42 @@ int owl_modmul(owl_plan* plan, int32_t* io_a, const int32_t* in_b, int mul3) {
   });
 }
 
+int owl_exp_mul(owl_plan* plan, int32_t* io_a, uint64_t h, const int32_t* in_b) {
+  return guarded([&] {
+    check_plan(plan);
+    check_buf(plan, io_a);
+    check_buf(plan, in_b);
+    if (io_a == in_b) { fail(OWL_ERR_ARG, "A and B must be different buffers"); }
+    DeviceGuard dg(plan->device);
+    if (h == 0) {
+      ck(cudaMemcpyAsync(io_a, in_b, (size_t)plan->N * sizeof(int32_t), cudaMemcpyDeviceToDevice, plan->stream),
+         "copy");
+      sync_and_check(plan);
+      return;
+    }
+    // left-to-right binary powering with the base's column spectrum kept in F2
+    pass1(plan, owl::P1_IN, plan->F2, io_a, 0);
+    pass2(plan, owl::P2_FWD, plan->F2, nullptr, plan->F2);
+    pass1(plan, owl::P1_IN, plan->F1, io_a, 0);
+    int top = 63;
+    while (!((h >> top) & 1)) { --top; }
+    for (int b = top - 1; b >= 0; --b) {
+      pass2(plan, owl::P2_SQUARE, plan->F1, nullptr, nullptr);
+      pass1(plan, owl::P1_FUSED, plan->F1, nullptr, 0);
+      if ((h >> b) & 1) {
+        pass2(plan, owl::P2_MUL, plan->F1, plan->F2, nullptr);
+        pass1(plan, owl::P1_FUSED, plan->F1, nullptr, 0);
+      }
+    }
+    // times B
+    pass1(plan, owl::P1_IN, plan->F2, const_cast<int32_t*>(in_b), 0);
+    pass2(plan, owl::P2_FWD, plan->F2, nullptr, plan->F2);
+    pass2(plan, owl::P2_MUL, plan->F1, plan->F2, nullptr);
+    pass1_out(plan, io_a, 0);
+    sync_and_check(plan);
+  });
+}
+
 int owl_is_equal(owl_plan* plan, const int32_t* a, const int32_t* b, int* equal) {
   return guarded([&] {
     check_plan(plan);

@@ -9,7 +9,9 @@
 // flags, this loop hands whole stretches between its stop points to
 // owl_square, which keeps the data in the FFT domain inside the stretch.
 #include <algorithm>
+#include <array>
 #include <cinttypes>
+#include <memory>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -21,6 +23,7 @@
 
 #include "owl.h"
 #include "owl_host.h"
+#include "owl_sha3.hpp"
 
 namespace fs = std::filesystem;
 
@@ -386,6 +389,33 @@ class HostGpu {
     return isEqual(check, aux);
   }
 
+  // reference Gpu::expMul(Buffer A, h, Buffer B): A := A^h * B
+  void expMul(int32_t* a, uint64_t h, const int32_t* b) { ck(owl_exp_mul(plan_, a, h, b)); }
+  // reference Gpu::expMul(Words A, h, Words B, doSquareB) (src/Gpu.cpp:839-847): A^h * (B or B^2)
+  Words expMul(const Words& A, uint64_t h, const Words& B, bool doSquareB) {
+    writeIn(check, B);
+    if (doSquareB) { squareLoop(check, check, 1); }
+    writeIn(data, A);
+    expMul(data, h, check);
+    return readOut(data);
+  }
+  // reference Gpu::expExp2 (src/Gpu.cpp:813-831): A^(2^n), in blocks of squarings
+  Words expExp2(const Words& A, uint32_t n) {
+    writeIn(data, A);
+    for (uint32_t k = 0; k < n;) {
+      const uint32_t its = std::min(1000u, n - k);
+      squareLoop(data, data, its);
+      k += its;
+    }
+    return readOut(data);
+  }
+  int32_t* allocBuf() {
+    int32_t* b = nullptr;
+    ck(owl_buf_alloc(plan_, &b));
+    return b;
+  }
+  void freeBuf(int32_t* b) { owl_buf_free(plan_, b); }
+
   void injectFault(int32_t* b) {
     uint32_t N = 0;
     ck(owl_plan_shape(plan_, &N, nullptr, nullptr));
@@ -403,6 +433,243 @@ class HostGpu {
   uint32_t E_;
   owl_plan* plan_ = nullptr;
 };
+
+// ---- PRP proofs (src/Proof.cpp, src/Proof.h) ----
+using Hash4 = std::array<uint64_t, 4>;
+
+Words make_words(uint32_t E, uint32_t v) {
+  Words w(n_words(E), 0);
+  w[0] = v;
+  return w;
+}
+// SHA3-256 of the first (E-1)/8+1 bytes of the words, optionally after a 32-byte prefix (src/Proof.cpp:22-28)
+Hash4 hash_words(uint32_t E, const Words& w) {
+  owl::Sha3_256 h;
+  h.update(w.data(), (E - 1) / 8 + 1);
+  return h.finish();
+}
+Hash4 hash_words(uint32_t E, const Hash4& prefix, const Words& w) {
+  owl::Sha3_256 h;
+  h.update(prefix.data(), sizeof(prefix));
+  h.update(w.data(), (E - 1) / 8 + 1);
+  return h.finish();
+}
+
+// "PRP PROOF\nVERSION=2\nHASHSIZE=64\nPOWER=%u\nNUMBER=M%u\n" + B + middles, (E-1)/8+1 bytes each
+// (src/Proof.h:42-49, src/Proof.cpp:62-86)
+constexpr const char* kProofHeader = "PRP PROOF\nVERSION=2\nHASHSIZE=64\nPOWER=%u\nNUMBER=M%u%c";
+
+struct Proof {
+  uint32_t E = 0;
+  Words B;
+  std::vector<Words> middles;
+
+  void save(const fs::path& path) const {
+    FILE* f = std::fopen(path.string().c_str(), "wb");
+    if (!f) { fail(OWL_ERR_ARG, "cannot write " + path.string()); }
+    FileCloser fc{f};
+    std::fprintf(f, kProofHeader, (unsigned)middles.size(), E, '\n');
+    const size_t nb = (E - 1) / 8 + 1;
+    bool ok = std::fwrite(B.data(), 1, nb, f) == nb;
+    for (const Words& w : middles) { ok = ok && std::fwrite(w.data(), 1, nb, f) == nb; }
+    if (!ok) { fail(OWL_ERR_ARG, "short write " + path.string()); }
+  }
+
+  static Proof load(const fs::path& path) {
+    FILE* f = std::fopen(path.string().c_str(), "rb");
+    if (!f) { fail(OWL_ERR_READ, "cannot open " + path.string()); }
+    FileCloser fc{f};
+    unsigned power = 0, E = 0;
+    char c = 0;
+    if (std::fscanf(f, kProofHeader, &power, &E, &c) != 3 || c != '\n' || power == 0 || power > 12 || E < 32) {
+      fail(OWL_ERR_READ, "invalid proof header");
+    }
+    const size_t nb = (E - 1) / 8 + 1;
+    auto readWords = [&]() {
+      Words w(n_words(E), 0);
+      if (std::fread(w.data(), 1, nb, f) != nb) { fail(OWL_ERR_READ, "truncated proof"); }
+      return w;
+    };
+    Proof p;
+    p.E = E;
+    p.B = readWords();
+    for (unsigned i = 0; i < power; ++i) { p.middles.push_back(readWords()); }
+    return p;
+  }
+
+  // src/Proof.cpp:88-128
+  bool verify(HostGpu& gpu, const std::vector<uint64_t>& hashes, bool* isPrime) const {
+    const uint32_t power = (uint32_t)middles.size();
+    *isPrime = (B == make_words(E, 9));
+    Words A = make_words(E, 3), Bw = B;
+    Hash4 hash = hash_words(E, Bw);
+    uint32_t span = E;
+    for (uint32_t i = 0; i < power; ++i, span = (span + 1) / 2) {
+      const Words& M = middles[i];
+      hash = hash_words(E, hash, M);
+      const uint64_t h = hash[0];
+      if (hashes.size() > i && h != hashes[i]) { return false; }
+      Bw = gpu.expMul(M, h, Bw, span % 2 != 0);
+      A = gpu.expMul(A, h, M, false);
+    }
+    A = gpu.expExp2(A, span);
+    return A == Bw;
+  }
+};
+
+// The residues a power-p proof needs (src/Proof.cpp:132-185): every sum of a subset of the
+// spans (E+1)/2, then halved (rounding up) p-1 times, with the empty sum replaced by E.
+std::vector<uint32_t> proof_points(uint32_t E, uint32_t power) {
+  std::vector<uint32_t> pts{0};
+  for (uint32_t p = 0, span = (E + 1) / 2; p < power; ++p, span = (span + 1) / 2) {
+    for (size_t i = 0, end = pts.size(); i < end; ++i) { pts.push_back(pts[i] + span); }
+  }
+  pts.front() = E;
+  std::sort(pts.begin(), pts.end());
+  return pts;
+}
+
+bool proof_in_points(uint32_t E, uint32_t power, uint32_t k) {  // src/Proof.cpp:187-200
+  if (k == E) { return true; }
+  uint32_t start = 0;
+  for (uint32_t p = 0, span = (E + 1) / 2; p < power; ++p, span = (span + 1) / 2) {
+    if (k > start + span) {
+      start += span;
+    } else if (k == start + span) {
+      return true;
+    }
+  }
+  return false;
+}
+
+class ProofSet {
+ public:
+  // residues live in <root>/<E>/proof/<k> (src/Proof.h:70), like the savefiles
+  ProofSet(const fs::path& root, uint32_t E, uint32_t power) : E(E), power(power), dir_(root / std::to_string(E) / "proof") {
+    if (power == 0 || power > 12) { fail(OWL_ERR_ARG, "invalid proof power"); }
+    fs::create_directories(dir_);
+    points_ = proof_points(E, power);
+    points_.push_back(UINT32_MAX);  // guard
+  }
+  const uint32_t E, power;
+
+  uint32_t next(uint32_t k) const { return *std::upper_bound(points_.begin(), points_.end(), k); }
+  uint32_t point(size_t i) const { return points_[i]; }
+
+  // file: u32 CRC32 of the words, then E/32+1 words (File::writeChecked, src/File.h:218-222)
+  void save(uint32_t k, const Words& w) const {
+    if (!k || k > E || !proof_in_points(E, power, k)) { fail(OWL_ERR_ARG, "not a proof point"); }
+    const fs::path tmp = file(k).string() + ".tmp";
+    {
+      FILE* f = std::fopen(tmp.string().c_str(), "wb");
+      if (!f) { fail(OWL_ERR_ARG, "cannot write " + tmp.string()); }
+      FileCloser fc{f};
+      const uint32_t crc = crc32(w);
+      if (std::fwrite(&crc, 4, 1, f) != 1 || std::fwrite(w.data(), 4, w.size(), f) != w.size()) {
+        fail(OWL_ERR_ARG, "short write " + tmp.string());
+      }
+    }
+    fs::rename(tmp, file(k));
+    if (load(k) != w) { fail(OWL_ERR_READ, "proof residue read-back differs"); }
+  }
+  Words load(uint32_t k) const {
+    FILE* f = std::fopen(file(k).string().c_str(), "rb");
+    if (!f) { fail(OWL_ERR_READ, "missing proof residue " + std::to_string(k)); }
+    FileCloser fc{f};
+    uint32_t crc = 0;
+    Words w(E / 32 + 1);
+    if (std::fread(&crc, 4, 1, f) != 1 || std::fread(w.data(), 4, w.size(), f) != w.size() || crc != crc32(w)) {
+      fail(OWL_ERR_READ, "bad proof residue " + std::to_string(k));
+    }
+    return w;
+  }
+  bool fileExists(uint32_t k) const {
+    std::error_code ec;
+    return fs::file_size(file(k), ec) == (uintmax_t)(E / 32 + 2) * 4 && !ec;
+  }
+  // every residue up to limitK is present, the last one readable (src/Proof.cpp:217-240)
+  bool isValidTo(uint32_t limitK) const {
+    auto it = std::upper_bound(points_.begin(), points_.end(), limitK);
+    if (it == points_.begin()) { return true; }
+    --it;
+    try {
+      load(*it);
+    } catch (const HostError&) {
+      return false;
+    }
+    while (it != points_.begin()) {
+      if (!fileExists(*--it)) { return false; }
+    }
+    return true;
+  }
+  // the largest power <= `power` whose residues up to k are all on disk (src/Proof.cpp:210-215)
+  static uint32_t effectivePower(const fs::path& root, uint32_t E, uint32_t power, uint32_t k) {
+    for (uint32_t p = power; p > 0; --p) {
+      if (ProofSet(root, E, p).isValidTo(k)) { return p; }
+    }
+    return 0;
+  }
+
+  // src/Proof.cpp:256-297: middles M_p folded from the residues with the running hashes
+  Proof computeProof(HostGpu& gpu, std::vector<uint64_t>& hashes) const {
+    Proof pr;
+    pr.E = E;
+    pr.B = load(E);
+    Hash4 hash = hash_words(E, pr.B);
+    std::vector<int32_t*> bufs;
+    for (uint32_t i = 0; i < power; ++i) { bufs.push_back(gpu.allocBuf()); }
+    struct Free {
+      HostGpu& g;
+      std::vector<int32_t*>& b;
+      ~Free() {
+        for (int32_t* x : b) { g.freeBuf(x); }
+      }
+    } freeBufs{gpu, bufs};
+    hashes.clear();
+    for (uint32_t p = 0; p < power; ++p) {
+      size_t it = 0;
+      const uint32_t s = 1u << (power - p - 1);
+      for (uint32_t i = 0; i < (1u << p); ++i) {
+        gpu.writeIn(bufs[it++], load(points_[s * (i * 2 + 1) - 1]));
+        for (uint32_t k = 0; i & (1u << k); ++k) {
+          --it;
+          gpu.expMul(bufs[it - 1], hashes[p - 1 - k], bufs[it]);
+        }
+      }
+      if (it != 1) { fail(OWL_ERR_ARG, "proof fold"); }
+      Words w = gpu.readOut(bufs[0]);
+      pr.middles.push_back(w);
+      hash = hash_words(E, hash, w);
+      hashes.push_back(hash[0]);
+    }
+    return pr;
+  }
+
+ private:
+  fs::path file(uint32_t k) const { return dir_ / std::to_string(k); }
+  fs::path dir_;
+  std::vector<uint32_t> points_;
+};
+
+// Gpu::saveProof (src/Gpu.cpp:1150-1166): generate into proof-tmp/, verify with the same hashes,
+// then move to proof/<E>-<power>.proof
+fs::path save_proof(HostGpu& gpu, const ProofSet& ps, const fs::path& root) {
+  for (int retry = 0; retry < 2; ++retry) {
+    std::vector<uint64_t> hashes;
+    Proof pr = ps.computeProof(gpu, hashes);
+    const std::string name = std::to_string(ps.E) + "-" + std::to_string(ps.power) + ".proof";
+    fs::create_directories(root / "proof-tmp");
+    fs::create_directories(root / "proof");
+    const fs::path tmp = root / "proof-tmp" / name, out = root / "proof" / name;
+    pr.save(tmp);
+    bool isPrime = false;
+    if (Proof::load(tmp).verify(gpu, hashes, &isPrime)) {
+      fs::rename(tmp, out);
+      return out;
+    }
+  }
+  fail(OWL_ERR_READ, "bad proof generation");
+}
 
 uint32_t baseCheckStep(uint32_t B) {  // src/Gpu.cpp:347-356
   switch (B) {
@@ -466,7 +733,7 @@ struct Log {
 
 uint32_t roundUp(uint32_t x, uint32_t m) { return ((x + m - 1) / m) * m; }
 
-// Gpu::isPrimePRP (src/Gpu.cpp:1400-1584) without proof generation.
+// Gpu::isPrimePRP (src/Gpu.cpp:1400-1584), with the proof residues and the proof at the end.
 void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
   const uint32_t B0 = o.block_size ? o.block_size : 1000;
   const uint32_t logStep = o.log_step ? o.log_step : 20000;
@@ -476,6 +743,8 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
   Log log{o};
   if (o.res_n) { *o.res_n = 0; }
   std::memset(&res, 0, sizeof(res));
+  if (o.proof_power && !o.save_dir) { fail(OWL_ERR_ARG, "a proof needs save_dir"); }
+  if (o.proof_power > 12) { fail(OWL_ERR_ARG, "invalid proof power"); }
 
   uint32_t nErrors = 0, nSeqErrors = 0;
   uint64_t lastFailedRes64 = 0;
@@ -504,6 +773,14 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
     const uint32_t checkStep = nErrors ? std::max(B, base / 2) : base;
     uint32_t k = st.k;
     const uint32_t startK = k, kEnd = E, kEndEnd = roundUp(kEnd, B);
+    // proof residues (src/Gpu.cpp:1428-1431, 1450, 1486-1493)
+    std::unique_ptr<ProofSet> proofSet;
+    if (o.proof_power) {
+      const uint32_t power = ProofSet::effectivePower(o.save_dir, E, o.proof_power, k);
+      if (power != o.proof_power) { log.line(fmt("Proof using power %u (vs %u)", power, o.proof_power)); }
+      if (power) { proofSet = std::make_unique<ProofSet>(o.save_dir, E, power); }
+    }
+    uint32_t persistK = proofSet ? proofSet->next(k) : UINT32_MAX;
     bool skipNextCheckUpdate = false;
     bool reload = false;
     Words finalWords;
@@ -516,8 +793,13 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
       // squarings up to the next point where the loop looks at the data
       uint32_t next = roundUp(k + 1, B);
       if (k < kEnd && kEnd < next) { next = kEnd; }
+      if (persistK > k && persistK < next) { next = persistK; }
       gpu.squareLoop(gpu.data, gpu.data, next - k);
       k = next;
+      if (k == persistK) {
+        proofSet->save(k, gpu.readOut(gpu.data));
+        persistK = proofSet->next(k);
+      }
       if (o.inject_fault_k && !injected && k >= o.inject_fault_k) {
         injected = true;
         gpu.injectFault(gpu.data);
@@ -552,6 +834,12 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
         if (k < kEnd && saver.enabled()) { saver.savePrp({E, k, B, r, rawCheck, nErrors, 0}); }
         log.line(fmt("OK %9u %016" PRIx64, k, r));
         if (k >= kEndEnd) {
+          if (proofSet) {
+            const fs::path pf = save_proof(gpu, *proofSet, o.save_dir);
+            res.proof_power = proofSet->power;
+            std::snprintf(res.proof_file, sizeof(res.proof_file), "%s", pf.string().c_str());
+            log.line("proof " + pf.string());
+          }
           res.finished = 1;
           res.k = k;
           res.n_errors = nErrors;
@@ -669,6 +957,32 @@ int owl_ll_run(int device, uint32_t E, const owl_run_opts* opts, owl_run_result*
   return guarded([&] {
     if (!opts || !out) { fail(OWL_ERR_ARG, "null argument"); }
     ll(device, E, *opts, *out);
+  });
+}
+
+void owl_sha3_256(const void* data, size_t size, uint8_t out[32]) {
+  owl::Sha3_256 h;
+  h.update(data, size);
+  owl::Sha3_256::digest_bytes(h.finish(), out);
+}
+
+int owl_proof_points(uint32_t E, uint32_t power, uint32_t* points, uint32_t cap, uint32_t* n) {
+  return guarded([&] {
+    if (power == 0 || power > 12 || E < 3 || !(E & 1)) { fail(OWL_ERR_ARG, "invalid exponent or proof power"); }
+    const std::vector<uint32_t> pts = proof_points(E, power);
+    if (n) { *n = (uint32_t)pts.size(); }
+    for (uint32_t i = 0; points && i < cap && i < pts.size(); ++i) { points[i] = pts[i]; }
+  });
+}
+
+int owl_proof_verify(int device, const char* proof_file, int* valid, int* is_prime) {
+  return guarded([&] {
+    if (!proof_file || !valid || !is_prime) { fail(OWL_ERR_ARG, "null argument"); }
+    const Proof pr = Proof::load(proof_file);
+    HostGpu gpu(device, pr.E, 0, 0);
+    bool prime = false;
+    *valid = pr.verify(gpu, {}, &prime) ? 1 : 0;
+    *is_prime = prime ? 1 : 0;
   });
 }
 

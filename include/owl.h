@@ -103,6 +103,10 @@ int owl_read_words(owl_plan* plan, const int32_t* buf, uint32_t* words);
 int owl_square(owl_plan* plan, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags);
 /* Gpu::modMul(ioA, inB, mul3) (src/Gpu.cpp:712-736): ioA := ioA * inB (* 3). */
 int owl_modmul(owl_plan* plan, int32_t* io_a, const int32_t* in_b, int mul3);
+/* A := A^h * B (reference Gpu::expMul on buffers, src/Gpu.cpp:833-837, with exponentiate's
+   left-to-right binary powering, 858-889): A's spectrum is kept while A is squared and multiplied
+   per bit of h. h = 0 gives A := B. A and B must differ. Used by proof generation and verification. */
+int owl_exp_mul(owl_plan* plan, int32_t* io_a, uint64_t h, const int32_t* in_b);
 /* Gpu::isEqual (src/Gpu.cpp:947-953, src/cl/etc.cl:34-41): digit-wise equality. */
 int owl_is_equal(owl_plan* plan, const int32_t* a, const int32_t* b, int* equal);
 /* Gpu::bufResidue (src/Gpu.cpp:955-975): res64 from the words around the wrap; falls

@@ -29,6 +29,8 @@ typedef struct {
   uint64_t* res_res64;    /* data res64 at that iteration */
   uint32_t* res_n;        /* number of checkpoints written */
   int split;              /* 1 = split-precision column pass (owl_plan_set_split; H = 2048 shapes only) */
+  uint32_t proof_power;   /* PRP: 0 = no proof; else save the 2^p proof residues under save_dir/<E>/proof/
+                             and write save_dir/proof/<E>-<p>.proof at the end (reference -proof p) */
 } owl_run_opts;
 
 typedef struct {
@@ -38,6 +40,9 @@ typedef struct {
   uint64_t res64;         /* final: PRP type-1 residue 3^(2^E)/9 (doDiv9, src/Gpu.cpp:1128-1148); LL value */
   uint32_t n_errors;      /* Gerbicz failures (each followed by a reload) */
   char res2048[513];      /* PRP: first 64 words of the type-1 residue, hex, most significant first */
+  uint32_t proof_power;   /* power of the proof written (may be lower than asked when resuming without
+                             the earlier residues, ProofSet::effectivePower), 0 = none */
+  char proof_file[1024];  /* path of the verified proof file, "" = none */
 } owl_run_result;
 
 /* PRP-3 test of 2^E - 1 (src/Gpu.cpp:1400-1584): resumes from save_dir/<E>/ when a savefile exists. */
@@ -55,6 +60,15 @@ int owl_ll_save(const char* save_dir, uint32_t E, uint32_t k, const uint32_t* da
 int owl_ll_load(const char* save_dir, uint32_t E, uint32_t* k, uint32_t* data, double* elapsed);
 /* CRC-32 (IEEE 802.3, reflected), the savefile checksum (src/common.cpp crc32) */
 uint32_t owl_crc32(const void* data, size_t size);
+
+/* SHA3-256 (FIPS 202) of size bytes, the proof hash (src/sha3.cpp through src/Sha3Hash.h) */
+void owl_sha3_256(const void* data, size_t size, uint8_t out[32]);
+/* The 2^power iterations whose residues a proof needs, increasing, the last = E
+   (ProofSet::ProofSet, src/Proof.cpp:132-185). *n = 2^power; cap may be smaller (then truncated). */
+int owl_proof_points(uint32_t E, uint32_t power, uint32_t* points, uint32_t cap, uint32_t* n);
+/* Proof::load + Proof::verify (src/Proof.cpp:72-128) on device `device`: *valid = the proof checks
+   out, *is_prime = its final residue is 9 (probable prime). OWL_ERR_READ on a malformed file. */
+int owl_proof_verify(int device, const char* proof_file, int* valid, int* is_prime);
 
 #ifdef __cplusplus
 }

@@ -262,6 +262,36 @@ def test_batch_of_uneven_exponents_matches_gmp(owl, oracle):
             p.close()
 
 
+def test_batch64_golden(owl):
+    """The 64-exponent batch (log-uniform in [1M, 20M], FFT at <= 19 bits/word) run as one graph per
+    1,000-iteration block: res64 after 1,000 and 2,000 iterations equal the GMP golden table."""
+    golden = load_golden("batch64")
+    if golden is None:
+        pytest.skip("golden table not generated")
+    plans = []
+    for it in golden["items"]:
+        _, W, H = owl.fft_choose(it["E"], 19.0)
+        plans.append(owl.Plan(it["E"], W=W, H=H))
+    try:
+        bufs = []
+        for p in plans:
+            b = p.alloc()
+            p.writeIn(b, small_words(p.E, 3))
+            bufs.append(b)
+        got = [[] for _ in plans]
+        with owl.Batch(plans) as batch:
+            for _ in range(2):
+                batch.square(bufs, 1000)
+                batch.sync()
+                for i, (p, b) in enumerate(zip(plans, bufs)):
+                    got[i].append("%016x" % p.bufResidue(b))
+        for it, g in zip(golden["items"], got):
+            assert g == it["res64"][:2], it["E"]
+    finally:
+        for p in plans:
+            p.close()
+
+
 def _pattern_words(E, N, pattern):
     """0: 3, 1: 2^E - 1, 2: every raw digit 2^(bits-1) - 1 (one carry runs through all digits),
     3: zero, 4: 2^E - 2, else random."""
