@@ -101,6 +101,14 @@ _SIGS = {
     "owl_proof_verify": ([ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
                          ctypes.c_int),
     "owl_exp_mul": ([_P, _P, ctypes.c_uint64, _P], ctypes.c_int),
+    "owl_worktodo_parse": ([ctypes.c_char_p, ctypes.c_void_p], ctypes.c_int),
+    "owl_worktodo_get": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p,
+                          ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "owl_task_run": ([ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                      ctypes.c_size_t], ctypes.c_int),
+    "owl_cert_run": ([ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint8),
+                      ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    "owl_file_md5": ([ctypes.c_char_p, ctypes.c_char_p], ctypes.c_int),
     "owl_batch_create": ([ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(_P), ctypes.POINTER(_P)], ctypes.c_int),
     "owl_batch_square": ([_P, ctypes.POINTER(_P), ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int),
     "owl_batch_sync": ([_P], ctypes.c_int),
@@ -326,6 +334,58 @@ def prp_run(E, device=0, block=1000, log_step=20000, check_step=0, stop_after=0,
     proof residues go to save_dir/<E>/proof/ and the verified proof to save_dir/proof/<E>-<p>.proof."""
     return _run("owl_prp_run", E, device, block, log_step, check_step, stop_after, save_dir, W, H,
                 inject_fault_k, verbose, split=split, proof_power=proof_power)
+
+
+class Task(ctypes.Structure):
+    """owl_task (include/owl_host.h): one worktodo entry."""
+    _fields_ = [("kind", ctypes.c_int), ("exponent", ctypes.c_uint32), ("squarings", ctypes.c_uint32),
+                ("aid", ctypes.c_char * 33), ("line", ctypes.c_char * 512)]
+    KINDS = {0: "PRP", 1: "LL", 2: "CERT"}
+
+    def as_dict(self):
+        return {"kind": self.KINDS.get(self.kind, "?"), "exponent": self.exponent, "squarings": self.squarings,
+                "aid": self.aid.decode(), "line": self.line.decode()}
+
+
+def worktodo_parse(line):
+    """The task of one worktodo line (reference Worktodo parse), or None if the line is ignored."""
+    t = Task()
+    if load().owl_worktodo_parse(line.encode(), ctypes.byref(t)) != 0:
+        return None
+    return t
+
+
+def worktodo_get(dir, instance=0, master_dir=None):
+    """Next task of worker `instance` from <dir>/worktodo-<instance>.txt or the pooled
+    <master_dir>/worktodo.txt, or None."""
+    t, found = Task(), ctypes.c_int(0)
+    _check(load().owl_worktodo_get(str(dir).encode(), instance, str(master_dir).encode() if master_dir else None,
+                                   ctypes.byref(t), ctypes.byref(found)))
+    return t if found.value else None
+
+
+def task_run(task, dir, instance=0, device=0, proof_power=0, block=1000, W=0, H=0, split=False):
+    """Runs one task (reference Task::execute); returns its result JSON line (also appended to
+    <dir>/results-<instance>.txt)."""
+    o = RunOpts(block, 0, 0, 0, 4, W, H, None, 0, 0, 0, None, None, None, 1 if split else 0, int(proof_power))
+    buf = ctypes.create_string_buffer(8192)
+    _check(load().owl_task_run(device, str(dir).encode(), instance, ctypes.byref(task), ctypes.byref(o), buf,
+                               len(buf)))
+    return buf.value.decode()
+
+
+def cert_run(E, squarings, cert_file, device=0):
+    """(sha3-256 digest bytes, res64) of `squarings` squarings of the start value in cert_file."""
+    out = (ctypes.c_uint8 * 32)()
+    r = ctypes.c_uint64(0)
+    _check(load().owl_cert_run(device, E, squarings, str(cert_file).encode(), out, ctypes.byref(r)))
+    return bytes(out), r.value
+
+
+def file_md5(path):
+    out = ctypes.create_string_buffer(33)
+    _check(load().owl_file_md5(str(path).encode(), out))
+    return out.value.decode()
 
 
 def sha3_256(data):

@@ -70,6 +70,35 @@ int owl_proof_points(uint32_t E, uint32_t power, uint32_t* points, uint32_t cap,
    out, *is_prime = its final residue is 9 (probable prime). OWL_ERR_READ on a malformed file. */
 int owl_proof_verify(int device, const char* proof_file, int* valid, int* is_prime);
 
+/* ---- work layer (src/Worktodo.cpp, src/Task.cpp) ---- */
+enum { OWL_TASK_PRP = 0, OWL_TASK_LL = 1, OWL_TASK_CERT = 2 }; /* reference Task::Kind PRP, LL, CERT */
+typedef struct {
+  int kind;               /* OWL_TASK_* */
+  uint32_t exponent;
+  uint32_t squarings;     /* CERT: squarings of the start value */
+  char aid[33];           /* assignment id (32 hex digits) or "" */
+  char line[512];         /* the verbatim worktodo line ("" for tasks not from a file) */
+} owl_task;
+
+/* One worktodo line (src/Worktodo.cpp:26-87): "PRP=", "PRPDC=" -> PRP; "Test=", "DoubleCheck=" -> LL;
+   "Cert=<aid>,1,2,E,-1,squarings" -> CERT. OWL_ERR_ARG for a line the reference ignores. */
+int owl_worktodo_parse(const char* line, owl_task* task);
+/* The next task for worker `instance`: the best line of <dir>/worktodo-<instance>.txt (the smallest CERT,
+   else the smallest exponent), else one moved from <master_dir>/worktodo.txt into the local file
+   (src/Worktodo.cpp:90-163). *found = 0 when there is no work. */
+int owl_worktodo_get(const char* dir, int instance, const char* master_dir, owl_task* task, int* found);
+/* Task::execute (src/Task.cpp:192-242): runs the task with opts (save_dir is set to dir), appends the
+   result JSON line to <dir>/results-<instance>.txt (writeResultPRP / LL / CERT, src/Task.cpp:141-190),
+   removes the task's line from <dir>/worktodo-<instance>.txt and copies the line to result. */
+int owl_task_run(int device, const char* dir, int instance, const owl_task* task, const owl_run_opts* opts,
+                 char* result, size_t result_len);
+/* Gpu::isCERT (src/Gpu.cpp:1665-1725): `squarings` squarings of the E-bit start value read from
+   cert_file ((E-1)/8+1 little-endian bytes), SHA3-256 of the result's bytes. */
+int owl_cert_run(int device, uint32_t E, uint32_t squarings, const char* cert_file, uint8_t sha3[32],
+                 uint64_t* res64);
+/* MD5 of a file as 32 lowercase hex digits (proof::fileHash, src/Proof.cpp:30-37) */
+int owl_file_md5(const char* path, char out[33]);
+
 #ifdef __cplusplus
 }
 #endif
