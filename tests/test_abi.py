@@ -9,12 +9,15 @@ import pytest
 
 from conftest import ROOT
 
-HEADER = os.path.join(ROOT, "include", "owl.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("owl.h", "owl_host.h")]
 
 
 def declared():
-    src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*|void)\s+(owl_\w+)\s*\(", src, re.M)))
+    names = set()
+    for h in HEADERS:
+        src = open(h).read()
+        names |= set(re.findall(r"^\s*(?:int|const char\*|void|uint32_t|uint64_t)\s+(owl_\w+)\s*\(", src, re.M))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
@@ -28,7 +31,9 @@ def lib():
 def test_header_declares_the_boundary():
     names = declared()
     for must in ("owl_plan_create", "owl_square", "owl_modmul", "owl_res64", "owl_read_words",
-                 "owl_write_words", "owl_is_equal", "owl_read_roe", "owl_probe_wait_timeout"):
+                 "owl_write_words", "owl_is_equal", "owl_read_roe", "owl_probe_wait_timeout", "owl_exp_mul",
+                 "owl_plan_set_split", "owl_prp_run", "owl_ll_run", "owl_proof_verify", "owl_task_run",
+                 "owl_cert_run", "owl_worktodo_get", "owl_sha3_256", "owl_crc32"):
         assert must in names
 
 
