@@ -101,6 +101,7 @@ _SIGS = {
     "owl_proof_verify": ([ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
                          ctypes.c_int),
     "owl_exp_mul": ([_P, _P, ctypes.c_uint64, _P], ctypes.c_int),
+    "owl_probe_tc_wait_timeout": ([_P], ctypes.c_int),
     "owl_worktodo_parse": ([ctypes.c_char_p, ctypes.c_void_p], ctypes.c_int),
     "owl_worktodo_get": ([ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p,
                           ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
@@ -307,6 +308,10 @@ class Plan:
     def probe_wait_timeout(self):
         """Returns the status of a device wait that must time out (ERR_TIMEOUT)."""
         return self.lib.owl_probe_wait_timeout(self.h)
+
+    def probe_tc_wait_timeout(self):
+        """Status of a tensor-core completion wait that must time out (ERR_TIMEOUT)."""
+        return self.lib.owl_probe_tc_wait_timeout(self.h)
 
 
 # ---- host drivers (include/owl_host.h) ----

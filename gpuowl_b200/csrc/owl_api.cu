@@ -1087,4 +1087,14 @@ int owl_probe_wait_timeout(owl_plan* plan) {
   });
 }
 
+int owl_probe_tc_wait_timeout(owl_plan* plan) {
+  return guarded([&] {
+    check_plan(plan);
+    DeviceGuard dg(plan->device);
+    owl::k_tc_wait_probe<<<1, 32, 0, plan->stream>>>(plan->args);
+    ck(cudaGetLastError(), "probe launch");
+    sync_and_check(plan);
+  });
+}
+
 }  // extern "C"

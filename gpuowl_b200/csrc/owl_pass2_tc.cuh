@@ -393,6 +393,15 @@ __global__ void __launch_bounds__(kTcH / 8, 2)
   ts_end(a, tslot);
 }
 
+// timeout probe of the tensor-core completion wait: an mbarrier that no MMA commit ever arrives on
+static __global__ void k_tc_wait_probe(Args a) {
+  OWL_SHARED(uint64_t, bar);
+  if (threadIdx.x == 0) { tc::mbar_init(&bar, 1); }
+  __syncthreads();
+  const bool ok = tc::mbar_wait(&bar, 0, a.timeoutNs);
+  if (!ok && threadIdx.x == 0) { atomicOr(&a.ctl->error, DEVERR_WAIT); }
+}
+
 }  // namespace owl
 
 #include <vector>

@@ -134,6 +134,9 @@ int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint
 /* Failure-detection probe: one device wait on a flag nothing sets, with the plan's
    timeout. Returns OWL_ERR_TIMEOUT (the expected outcome) and leaves the plan usable. */
 int owl_probe_wait_timeout(owl_plan* plan);
+/* Test hook of the split-precision pass's completion wait: waits on an mbarrier that nothing
+   arrives on, with the plan's timeout; returns OWL_ERR_TIMEOUT and leaves the plan usable. */
+int owl_probe_tc_wait_timeout(owl_plan* plan);
 
 /* Batches of exponents (BASELINE "batched uneven exponents"; the reference runs 1-4 independent
    workers, each with its own in-order queue, src/main.cpp:111-118). A batch groups plans of one

@@ -73,3 +73,18 @@ def test_split_rejects_other_heights(owl):
         with pytest.raises(owl.OwlError) as e:
             p.set_split(True)
         assert e.value.status == -1
+
+
+def test_tc_wait_timeout_probe_keeps_plan_usable(owl, oracle):
+    """The tensor-core completion wait is bounded: a barrier nothing arrives on times out with
+    ERR_TIMEOUT after the plan's limit, and the plan still computes in the split form."""
+    E = 4700021
+    with owl.Plan(E, W=64, H=2048, split=True) as p:
+        p.set_timeout(20_000_000)  # 20 ms
+        assert p.probe_tc_wait_timeout() == owl.ERR_TIMEOUT
+        p.set_timeout(2_000_000_000)
+        a = p.alloc()
+        w = random_words(E, 77)
+        p.writeIn(a, w)
+        p.squareLoop(a, a, 3)
+        assert np.array_equal(p.readOut(a), oracle.gmp_square(E, w, 3))
