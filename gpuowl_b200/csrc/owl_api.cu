@@ -427,8 +427,8 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   const std::vector<owl::HostC> twHtc = tcShape ? owl::stage_tables(H, 8, owl::kTcR1) : std::vector<owl::HostC>();
   const std::vector<uint8_t> tcB = tcShape ? owl::tc_dft_digits() : std::vector<uint8_t>();
   size_t nC = t.twW.size() + t.twH.size() + t.rootH.size() + t.twLo.size() + t.twHi.size() + twHtc.size();
-  size_t bytes = 256 * 15 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
-                 (t.x1.size() + t.x2.size()) * sizeof(uint32_t) + tcB.size();
+  size_t bytes = 256 * 16 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
+                 (t.x1.size() + t.x2.size() + t.p1masks.size()) * sizeof(uint32_t) + tcB.size();
   ck(cudaMalloc(&p->tableMem, bytes), "cudaMalloc(tables)");
   std::vector<char> host(bytes, 0);
   char* hcur = host.data();
@@ -450,6 +450,7 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   p->args.wt2 = reinterpret_cast<const double*>(dbase + put(t.wt2.data(), t.wt2.size() * sizeof(double)));
   p->args.iwt2 = reinterpret_cast<const double*>(dbase + put(t.iwt2.data(), t.iwt2.size() * sizeof(double)));
   p->args.x2 = reinterpret_cast<const uint32_t*>(dbase + put(t.x2.data(), t.x2.size() * sizeof(uint32_t)));
+  p->args.p1masks = reinterpret_cast<const uint2*>(dbase + put(t.p1masks.data(), t.p1masks.size() * sizeof(uint32_t)));
   if (tcShape) {
     p->twHtc = reinterpret_cast<const C*>(dbase + put(twHtc.data(), twHtc.size() * sizeof(C)));
     p->tcB = reinterpret_cast<const unsigned char*>(dbase + put(tcB.data(), tcB.size()));

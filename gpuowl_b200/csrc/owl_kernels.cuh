@@ -48,6 +48,8 @@ struct Args {
   const double* wt2;   // per (line j2, e): 2^(X2/N)
   const double* iwt2;  // per (line j2, e): 2^(-X2/N) / (4 hN)
   const uint32_t* x2;  // per (line j2, e): X2 = step*(2 j2 + e) mod N
+  const uint2* p1masks; // per (line group g, pass-1 thread t): the big-word and wrap bits of the thread's
+                        // 32 words, bit (r R + ll) 2 + e for column t + (W/RL) r, line g R + ll, word e
   long long* shuttle;  // carry rows, (H/R) x W
   long long* pending;  // (word index, carry) pairs, kPendingCap entries
   uint32_t* flags;     // per line group
@@ -174,6 +176,8 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   }
 
   const unsigned long long pol = l2_keep_policy();
+  // word classes of this thread's 32 words (fixed per shape, tabulated on the host)
+  const uint2 wmask = __ldg(a.p1masks + (size_t)g * T + t);
   // per-line mapping for the inner stages
   const int l = t % R;
   const int tl = t / R;
@@ -242,12 +246,11 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   // (the exit mode must produce the canonical balanced digits).
   double dg[R][RL][2];
   long long dig[R][RL][2];
-  uint32_t bigmask = 0;   // bit (r*R + ll)*2 + e: word is big
-  uint32_t wrapmask = 0;  // bit (r*R + ll)*2 + e: X1 + X2 >= N (weight halved)
+  const uint32_t bigmask = wmask.x;   // bit (r*R + ll)*2 + e: word is big
+  const uint32_t wrapmask = wmask.y;  // bit (r*R + ll)*2 + e: X1 + X2 >= N (weight halved)
 #pragma unroll
   for (int r = 0; r < RL; ++r) {
     const uint32_t j1 = t + (W / RL) * r;
-    const uint32_t X1 = __ldg(a.x1 + j1);
     if constexpr (MODE == P1_IN) {
       // digits in natural word order: word 2(H j1 + j2) + e
 #pragma unroll
@@ -256,10 +259,6 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
         int2 w2 = *reinterpret_cast<const int2*>(words + 2 * ((size_t)a.H * j1 + j2));
         dg[ll][r][0] = (double)w2.x;
         dg[ll][r][1] = (double)w2.y;
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          if (X1 + __ldg(a.x2 + 2 * j2 + e) >= a.N) { wrapmask |= 1u << ((r * R + ll) * 2 + e); }
-        }
       }
     } else {
       const double iw1 = __ldg(a.iwt1 + j1);
@@ -273,13 +272,8 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int bit = (r * R + ll) * 2 + e;
-          uint32_t X2 = __ldg(a.x2 + 2 * j2 + e);
-          uint32_t sum = X1 + X2;
-          bool wrap = sum >= a.N;
-          uint32_t extra = wrap ? sum - a.N : sum;
-          bool big = extra < a.eModN;
-          if (big) { bigmask |= 1u << bit; }
-          if (wrap) { wrapmask |= 1u << bit; }
+          const bool wrap = (wrapmask >> bit) & 1u;
+          const bool big = (bigmask >> bit) & 1u;
           double iw = iw1 * __ldg(a.iwt2 + 2 * j2 + e);
           if (wrap) { iw *= 2.0; }
           double x = e ? z.y : z.x;

@@ -56,7 +56,7 @@ size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // byte layout of the scratch for one shape; returns the total size
 struct Layout {
-  size_t F, shuttle, pending, flags, ctl, roe, twW, twH, rootH, twLo, twHi, wt1, iwt1, x1, wt2, iwt2, x2, total;
+  size_t F, shuttle, pending, flags, ctl, roe, twW, twH, rootH, twLo, twHi, wt1, iwt1, x1, wt2, iwt2, x2, masks, total;
 };
 Layout layout(uint32_t W, uint32_t H, uint32_t loShift) {
   const uint32_t hN = W * H, G = H / kR;
@@ -81,6 +81,7 @@ Layout layout(uint32_t W, uint32_t H, uint32_t loShift) {
   L.wt2 = take(2 * H * sizeof(double));
   L.iwt2 = take(2 * H * sizeof(double));
   L.x2 = take(2 * H * sizeof(uint32_t));
+  L.masks = take((size_t)G * (kR * W / 16) * sizeof(uint2));
   L.total = o;
   return L;
 }
@@ -131,6 +132,29 @@ __global__ void k_noalloc_tables(owl::Args a, uint32_t twWn, uint32_t twHn) {
     const_cast<uint32_t*>(a.x2)[i] = X;
     const_cast<double*>(a.wt2)[i] = exp2((double)X / N);
     const_cast<double*>(a.iwt2)[i] = exp2(-(double)X / N) / (4.0 * (double)a.hN);
+  }
+  // pass-1 word classes (the host-side word_masks, from the same X1 / X2 formulas)
+  {
+    constexpr uint32_t RL = 16 / kR;
+    const uint32_t T = kR * W / 16, G = H / kR;
+    for (uint32_t i = tid; i < G * T; i += nth) {
+      const uint32_t g = i / T, th = i % T;
+      uint32_t big = 0, wrap = 0;
+      for (uint32_t r = 0; r < RL; ++r) {
+        const uint32_t j1 = th + (W / RL) * r;
+        const uint32_t X1 = (uint32_t)((step * 2 * H * (uint64_t)j1) % N);
+        for (uint32_t ll = 0; ll < kR; ++ll) {
+          for (uint32_t e = 0; e < 2; ++e) {
+            const uint32_t bit = (r * kR + ll) * 2 + e;
+            const uint32_t X = X1 + (uint32_t)((step * (uint64_t)(2 * (g * kR + ll) + e)) % N);
+            const bool w = X >= N;
+            if (w) { wrap |= 1u << bit; }
+            if ((w ? X - N : X) < a.E % N) { big |= 1u << bit; }
+          }
+        }
+      }
+      const_cast<uint2*>(a.p1masks)[i] = make_uint2(big, wrap);
+    }
   }
   for (uint32_t i = tid; i < H / kR; i += nth) { a.flags[i] = 0; }
   if (tid == 0) {
@@ -236,6 +260,7 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
   a.wt2 = reinterpret_cast<const double*>(base + L.wt2);
   a.iwt2 = reinterpret_cast<const double*>(base + L.iwt2);
   a.x2 = reinterpret_cast<const uint32_t*>(base + L.x2);
+  a.p1masks = reinterpret_cast<const uint2*>(base + L.masks);
   a.shuttle = reinterpret_cast<long long*>(base + L.shuttle);
   a.pending = reinterpret_cast<long long*>(base + L.pending);
   a.flags = reinterpret_cast<uint32_t*>(base + L.flags);

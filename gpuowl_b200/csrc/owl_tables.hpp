@@ -82,6 +82,7 @@ struct Tables {
   std::vector<HostC> twW, twH, rootH, twLo, twHi;
   std::vector<double> wt1, iwt1, wt2, iwt2;
   std::vector<uint32_t> x1, x2;
+  std::vector<uint32_t> p1masks;  // (bigmask, wrapmask) per (line group, pass-1 thread)
 };
 
 // lines per pass-1 block; the width FFT's cross-line radix is 16 / kLinesPerBlock
@@ -120,6 +121,36 @@ inline bool shape_for(uint32_t n, uint32_t* W, uint32_t* H) {
     }
   }
   return found;
+}
+
+// The big-word and wrap bits of every pass-1 thread's words: thread t of line group g holds
+// column j1 = t + (W/RL) r (r < RL = 16/R) of lines j2 = g R + ll (ll < R), words e = 0, 1;
+// bit (r R + ll) 2 + e. With X = X1[j1] + X2[2 j2 + e], the weight wraps when X >= N and the
+// word is big when X mod N < E mod N.
+inline std::vector<uint32_t> word_masks(uint32_t E, uint32_t W, uint32_t H, const uint32_t* x1, const uint32_t* x2) {
+  const uint32_t R = kLinesPerBlock, RL = 16 / R, T = R * W / 16, G = H / R, N = 2 * W * H;
+  std::vector<uint32_t> m(2 * (size_t)G * T);
+  for (uint32_t g = 0; g < G; ++g) {
+    for (uint32_t th = 0; th < T; ++th) {
+      uint32_t big = 0, wrap = 0;
+      for (uint32_t r = 0; r < RL; ++r) {
+        const uint32_t j1 = th + (W / RL) * r;
+        for (uint32_t ll = 0; ll < R; ++ll) {
+          const uint32_t j2 = g * R + ll;
+          for (uint32_t e = 0; e < 2; ++e) {
+            const uint32_t bit = (r * R + ll) * 2 + e;
+            const uint32_t X = x1[j1] + x2[2 * j2 + e];
+            const bool w = X >= N;
+            if (w) { wrap |= 1u << bit; }
+            if ((w ? X - N : X) < E % N) { big |= 1u << bit; }
+          }
+        }
+      }
+      m[2 * ((size_t)g * T + th)] = big;
+      m[2 * ((size_t)g * T + th) + 1] = wrap;
+    }
+  }
+  return m;
 }
 
 inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
@@ -163,6 +194,7 @@ inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
     t.wt2[i] = (double)exp2l((long double)X / N);
     t.iwt2[i] = (double)(exp2l(-(long double)X / N) * norm);
   }
+  t.p1masks = word_masks(E, W, H, t.x1.data(), t.x2.data());
   return t;
 }
 

@@ -73,6 +73,7 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   a.wt2 = p.t.wt2.data();
   a.iwt2 = p.t.iwt2.data();
   a.x2 = p.t.x2.data();
+  a.p1masks = reinterpret_cast<const uint2*>(p.t.p1masks.data());
   a.shuttle = p.shuttle.data();
   a.pending = p.pending.data();
   a.flags = p.flags.data();

@@ -36,6 +36,10 @@ struct double2 {
 struct int2 {
   int x, y;
 };
+struct uint2 {
+  unsigned x, y;
+};
+inline uint2 make_uint2(unsigned x, unsigned y) { return uint2{x, y}; }
 inline double2 make_double2(double x, double y) { return double2{x, y}; }
 inline int2 make_int2(int x, int y) { return int2{x, y}; }
 
