@@ -334,7 +334,7 @@ def run_ours(args, rank, world, local):
                                 "frac": round(tc_ops / (tc_ms * 1e-3) / 1e12 / (2 * bf16[0]), 4),
                                 "peak_kind": "2 x %s bf16 dense (int8 dense rate is twice bf16's)" % bf16[1],
                                 "int8_ops_per_launch": tc_ops},
-            "gpu_launches": (5 + 2 * B + 1) * args.steps,
+            "gpu_launches": (2 * B + 8) * args.steps,
             "clocks": split["clocks"],
             "vs_plain": round(s_value / value, 3),
         }
@@ -363,7 +363,9 @@ def run_ours(args, rank, world, local):
                "sample": "%d squarings at E=%d, N=8M with oracle/ibdwt.c (OpenMP, all host threads)"
                          % (iters, E_8M)}
 
-    launches_per_step = 5 + 2 * B + 1
+    # per timed step: modMul = pass1 IN, pass2 FWD, pass1 IN, pass2 MUL, pass1 OUT, carry fixup (6);
+    # the block = pass1 IN, B x pass2, B-1 x pass1 FUSED, pass1 OUT, carry fixup (2B + 2)
+    launches_per_step = 2 * B + 8
     line = {
         "metric": "ms/iter PRP @8M FFT: split-precision TC vs plain FP64, bit-exact res64",
         "value": round(value, 5), "unit": "ms/iter", "n_gpus": world, "steps": args.steps,
