@@ -160,6 +160,12 @@ def fft_choose(E, max_bpw=0.0, tune=None):
         import json
         with open(tune) as f:
             t = json.load(f)
+        # with measured max bits/word (tune --bpw-scan): the smallest FFT whose limit covers E
+        # (or max_bpw when given)
+        scanned = sorted((int(n), v) for n, v in t.items() if len(v) >= 5 and v[4])
+        for n, v in scanned:
+            if E / n <= (max_bpw if max_bpw > 0 else v[4]):
+                return n, int(v[0]), int(v[1])
         if str(N.value) in t:
             return N.value, int(t[str(N.value)][0]), int(t[str(N.value)][1])
     return N.value, W.value, H.value

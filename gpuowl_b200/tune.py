@@ -88,6 +88,61 @@ def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True, five=False
     return rows
 
 
+def roe_at(N, W, H, bpw, iters, device=0):
+    """Max round-off of `iters` squarings of a random residue at E = N * bpw (odd) on W x H."""
+    import numpy as np
+    import gpuowl_b200 as owl
+    E = next_odd_exponent(N * bpw)
+    with owl.Plan(E, device=device, W=W, H=H) as p:
+        b = p.alloc()
+        rng = np.random.default_rng(E)
+        w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
+        if E % 32:
+            w[-1] &= (1 << (E % 32)) - 1
+        p.writeIn(b, w)
+        p.squareLoop(b, b, 20)
+        p.readROE()
+        done = 0
+        while done < iters:
+            n = min(1000, iters - done)
+            p.squareLoop(b, b, n)
+            done += n
+        return float(p.readROE().max())
+
+
+def bpw_scan(shapes, iters, limit=0.3, start=16.0, step=0.25, device=0, verbose=True):
+    """The reference's BPW table (src/fftbpw.h, measured by its -ztune) for this build's FFTs:
+    for each (N, W, H) the largest bits per word, on a `step` grid from `start`, whose max round-off
+    over `iters` squarings stays below `limit`. Returns {N: (W, H, max_bpw, [(bpw, roe), ...])}."""
+    from gpuowl_b200 import build
+    build.build()
+    out = {}
+    for (N, W, H) in shapes:
+        curve, best = [], None
+        bpw = start
+        while bpw <= 21.0:
+            roe = roe_at(N, W, H, bpw, iters, device)
+            curve.append((bpw, roe))
+            if verbose:
+                print("N=%-9d %-14s bpw %.2f  max ROE %.4f" % (N, spec(W, H), bpw, roe), flush=True)
+            if roe >= limit:
+                break
+            best = bpw
+            bpw += step
+        out[N] = (W, H, best, curve)
+    return out
+
+
+def write_bpw(table, limit, iters, out_txt):
+    with open(out_txt, "w") as f:
+        f.write("# max bits/word with max ROE < %.2f over %d squarings of a random residue\n" % (limit, iters))
+        f.write("# N  spec  max_bpw  (bpw:roe ...)\n")
+        for N in sorted(table):
+            W, H, best, curve = table[N]
+            f.write("%9d %14s %6s  %s\n" % (N, spec(W, H), "%.2f" % best if best else "-",
+                                           " ".join("%.2f:%.3f" % c for c in curve)))
+
+
 def write(rows, max_bpw, out_txt, out_json):
     lines, prev_cost = [], 0.0
     for N in sorted(rows):
@@ -110,7 +165,23 @@ def main():
     ap.add_argument("--out", default="tune.txt")
     ap.add_argument("--json", default="tune.json")
     ap.add_argument("--five", action="store_true", help="also the 5 * 2^k FFT lengths")
+    ap.add_argument("--bpw-scan", metavar="TUNE_JSON", help="measure the max bits/word of the shapes in TUNE_JSON")
+    ap.add_argument("--roe-limit", type=float, default=0.3)
     a = ap.parse_args()
+    if a.bpw_scan:
+        with open(a.bpw_scan) as f:
+            t = json.load(f)
+        shapes = [(int(N), v[0], v[1]) for N, v in t.items()
+                  if (1 << a.min_lg) <= int(N) <= (1 << a.max_lg)]
+        table = bpw_scan(sorted(shapes), a.iters, a.roe_limit)
+        write_bpw(table, a.roe_limit, a.iters, a.out)
+        for N, (W, H, best, _) in table.items():
+            if best and str(N) in t:
+                t[str(N)] = list(t[str(N)][:4]) + [best]
+        with open(a.json, "w") as f:
+            json.dump(t, f, indent=1)
+        print(open(a.out).read())
+        return
     rows = tune(a.min_lg, a.max_lg, a.iters, a.bpw, five=a.five)
     write(rows, a.bpw, a.out, a.json)
     print(open(a.out).read())
