@@ -97,3 +97,17 @@ def test_tune_file_format(tmp_path):
     lines = open(tmp_path / "tune.txt").read().splitlines()
     assert lines[0] == "%6.1f %14s # %u" % (21.3, "256:2:256", 4718592)
     assert lines[1].split()[1] == "2K:2:1K"
+
+
+def test_fft_choose_with_measured_bpw_table(lib, tmp_path):
+    """With a tune file that carries measured max bits/word, the smallest FFT whose limit covers E
+    is chosen (reference FFTConfig::bestFit over fftbpw.h)."""
+    import json
+    import gpuowl_b200 as g
+    t = {str(1 << 23): [2048, 2048, 114.2, 0.15, 18.0], str(5 << 22): [4096, 2560, 391.1, 0.24, 17.75],
+         str(1 << 24): [4096, 2048, 259.8, 0.22, 17.75]}
+    p = tmp_path / "tune.json"
+    p.write_text(json.dumps(t))
+    assert g.fft_choose(150000001, tune=str(p)) == (1 << 23, 2048, 2048)     # 17.9 bits/word
+    assert g.fft_choose(152000001, tune=str(p)) == (1 << 24, 4096, 2048)     # 18.1 > 18.0 at 8M
+    assert g.fft_choose(333000017, tune=str(p)) == (5 << 22, 4096, 2560)     # 19.8 at 16M, 15.9 at 20M
