@@ -112,7 +112,7 @@ def test_emulated_split_precision_column_pass(emu, oracle, mode):
     assert 0 < float(lines[0].split()[1]) < 0.1
 
 
-@pytest.mark.parametrize("E,N,pattern", [(216091, 16384, p) for p in range(6)] + [(1300021, 81920, 2)])
+@pytest.mark.parametrize("E,N,pattern", [(216091, 16384, p) for p in range(6)] + [(327691, 20480, 2)])
 def test_emulated_device_expand_compact(emu, E, N, pattern):
     """owl_pack.cuh kernels against owl_words.hpp (3, 2^E-1, an all-propagating carry, 0, 2^E-2, random)."""
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")
