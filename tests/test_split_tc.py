@@ -88,3 +88,25 @@ def test_tc_wait_timeout_probe_keeps_plan_usable(owl, oracle):
         p.writeIn(a, w)
         p.squareLoop(a, a, 3)
         assert np.array_equal(p.readOut(a), oracle.gmp_square(E, w, 3))
+
+
+def test_split_plans_in_one_batch(owl, oracle):
+    """Two split-form plans (different widths) squared as one batch graph, against GMP."""
+    exps = [(4700021, 64, 2048), (9400013, 128, 2048)]
+    plans = [owl.Plan(E, W=W, H=H, split=True) for (E, W, H) in exps]
+    try:
+        bufs, starts = [], []
+        for p in plans:
+            b = p.alloc()
+            w = random_words(p.E, p.E + 5)
+            p.writeIn(b, w)
+            bufs.append(b)
+            starts.append(w)
+        with owl.Batch(plans) as batch:
+            batch.square(bufs, 17)
+            batch.sync()
+        for p, b, w in zip(plans, bufs, starts):
+            assert np.array_equal(p.readOut(b), oracle.gmp_square(p.E, w, 17)), p.E
+    finally:
+        for p in plans:
+            p.close()
