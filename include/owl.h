@@ -139,7 +139,7 @@ int owl_probe_wait_timeout(owl_plan* plan);
    arrives on, with the plan's timeout; returns OWL_ERR_TIMEOUT and leaves the plan usable. */
 int owl_probe_tc_wait_timeout(owl_plan* plan);
 
-/* Batches of exponents (BASELINE "batched uneven exponents"; the reference runs 1-4 independent
+/* Batches of exponents of uneven FFT lengths (the reference runs 1-4 independent
    workers, each with its own in-order queue, src/main.cpp:111-118). A batch groups plans of one
    device, each with its own exponent and FFT shape; owl_batch_square runs n squarings of every
    plan's buffer as ONE CUDA-graph launch (one fork-join graph, a branch per plan, captured on
