@@ -88,7 +88,7 @@ struct Tables {
 // lines per pass-1 block; the width FFT's cross-line radix is 16 / kLinesPerBlock
 constexpr uint32_t kLinesPerBlock = 2;
 
-// Shapes this build supports: W a power of two in [64, 4096]; H a power of two in
+// Shapes the library supports: W a power of two in [64, 4096]; H a power of two in
 // [64, 4096], or 5 * 2^k in {640, 1280, 2560} (a radix-5 stage in the column FFT).
 inline bool h_supported(uint32_t H) {
   return (is_pow2(H) && H >= 64 && H <= 4096) || H == 640 || H == 1280 || H == 2560;

@@ -3,7 +3,7 @@ each FFT with Gpu::timePRP and writes tune.txt).
 
     python -m gpuowl_b200.tune [--min-lg 13] [--max-lg 23] [--iters 200] [--out tune.txt]
 
-For every FFT size N = 2^lg, and N = 5 * 2^(lg-3) with --five, it times each W x H split this build
+For every FFT size N = 2^lg, and N = 5 * 2^(lg-3) with --five, it times each W x H split the library
 supports (W a power of two in [64, 4096]; H a power of two in [64, 4096] with H/W in {1/2, 1, 2, 4},
 or H in {640, 1280, 2560}) with owl_profile_square (device time of the two passes per
 squaring, at an exponent of 18 bits per word), keeps the fastest split, and records its max
@@ -111,7 +111,7 @@ def roe_at(N, W, H, bpw, iters, device=0):
 
 
 def bpw_scan(shapes, iters, limit=0.3, start=16.0, step=0.25, device=0, verbose=True):
-    """The reference's BPW table (src/fftbpw.h, measured by its -ztune) for this build's FFTs:
+    """The reference's BPW table (src/fftbpw.h, measured by its -ztune) for this library's FFTs:
     for each (N, W, H) the largest bits per word, on a `step` grid from `start`, whose max round-off
     over `iters` squarings stays below `limit`. Returns {N: (W, H, max_bpw, [(bpw, roe), ...])}."""
     from gpuowl_b200 import build
