@@ -256,9 +256,11 @@ class Plan:
         assert w.size == self.nwords
         _check(self.lib.owl_write_words(self.h, buf, w.ctypes.data_as(_U32P)))
 
-    def readOut(self, buf):
-        """Compact words of a buffer (reference readAndCompress: checked read + compactBits)."""
-        w = np.empty(self.nwords, dtype=np.uint32)
+    def readOut(self, buf, out=None):
+        """Compact words of a buffer (reference readAndCompress: checked read + compactBits), into
+        `out` (a contiguous uint32 array of nwords, e.g. over pinned memory) when given."""
+        w = np.empty(self.nwords, dtype=np.uint32) if out is None else out
+        assert w.dtype == np.uint32 and w.size == self.nwords and w.flags["C_CONTIGUOUS"]
         _check(self.lib.owl_read_words(self.h, buf, w.ctypes.data_as(_U32P)))
         return w
 
