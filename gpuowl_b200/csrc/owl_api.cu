@@ -135,8 +135,9 @@ template <int W, int M> void setp1attr() {
      "cudaFuncSetAttribute(pass1)");
 }
 template <int H, int M> void setp2attr() {
-  size_t sm = 2 * (size_t)owl::p2_col_stride<H>() * sizeof(C);
-  ck(cudaFuncSetAttribute(owl::k_pass2<H, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+  constexpr int V = owl::p2_vpt(H);
+  size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
+  ck(cudaFuncSetAttribute(owl::k_pass2<H, kR, M, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
      "cudaFuncSetAttribute(pass2)");
 }
 
@@ -179,18 +180,19 @@ template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int 
 }
 
 template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts) {
-  constexpr int T = H / 8;
-  size_t sm = 2 * (size_t)owl::p2_col_stride<H>() * sizeof(C);
+  constexpr int V = owl::p2_vpt(H);
+  constexpr int T = 2 * H / V;
+  size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
   dim3 grid(p->W / 2);
   switch (mode) {
     case owl::P2_SQUARE:
-      owl::k_pass2<H, kR, owl::P2_SQUARE><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
+      owl::k_pass2<H, kR, owl::P2_SQUARE, V><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
       break;
     case owl::P2_FWD:
-      owl::k_pass2<H, kR, owl::P2_FWD><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
+      owl::k_pass2<H, kR, owl::P2_FWD, V><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
       break;
     default:
-      owl::k_pass2<H, kR, owl::P2_MUL><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
+      owl::k_pass2<H, kR, owl::P2_MUL, V><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
       break;
   }
 }

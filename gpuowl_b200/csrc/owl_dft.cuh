@@ -206,25 +206,27 @@ template <int PS> __device__ __forceinline__ int pad(int i) { return i + (i >> P
 
 constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x / 2); }
 
-// ---- Stockham stage helpers for one line of N complex values held by N/16
-// threads, 16 values per thread. Stage radix R (R divides 16): thread `tl`
-// runs butterflies j = tl + (N/16) b, b < 16/R, inputs x[j + r N/R],
+// ---- Stockham stage helpers for one line of N complex values held by N/VPT
+// threads, VPT (16 or 8) values per thread. Stage radix R (R divides VPT, or 5):
+// thread `tl` runs butterflies j = tl + (N/VPT) b, b < VPT/R, inputs x[j + r N/R],
 // twiddle w_(NS R)^(r (j mod NS)), outputs y[(j/NS) NS R + j mod NS + r NS].
 
 // butterflies per thread of a radix-R stage (radix 5 leaves the last one to some threads only)
-template <int R> constexpr int st_nb() { return (16 + R - 1) / R; }
-template <int R, int N> __device__ __forceinline__ bool st_has(int j) { return (16 % R == 0) || j < N / R; }
+template <int R, int VPT = 16> constexpr int st_nb() { return (VPT + R - 1) / R; }
+template <int R, int N, int VPT = 16> __device__ __forceinline__ bool st_has(int j) {
+  return (VPT % R == 0) || j < N / R;
+}
 // j mod NS and j / NS for j >= 0 (mask and shift when NS is a power of two)
 template <int NS> __device__ __forceinline__ int smod(int j) {
   if constexpr ((NS & (NS - 1)) == 0) { return j & (NS - 1); } else { return (int)((unsigned)j % (unsigned)NS); }
 }
 template <int NS> __device__ __forceinline__ int sdiv(int j) { return (int)((unsigned)j / (unsigned)NS); }
 
-template <int R, int N, int PS> __device__ __forceinline__ void st_load(const C* buf, int tl, C* v) {
+template <int R, int N, int PS, int VPT = 16> __device__ __forceinline__ void st_load(const C* buf, int tl, C* v) {
 #pragma unroll
-  for (int b = 0; b < st_nb<R>(); ++b) {
-    int j = tl + (N / 16) * b;
-    if (!st_has<R, N>(j)) { continue; }
+  for (int b = 0; b < st_nb<R, VPT>(); ++b) {
+    int j = tl + (N / VPT) * b;
+    if (!st_has<R, N, VPT>(j)) { continue; }
 #pragma unroll
     for (int r = 0; r < R; ++r) { v[b * R + r] = buf[pad<PS>(j + r * (N / R))]; }
   }
@@ -236,12 +238,13 @@ template <int R, int N, int PS> __device__ __forceinline__ void st_load(const C*
 // within a few ulp), which keeps the L1 data path free for the exchanges.
 template <bool INV> __device__ __forceinline__ void twmul(C& v, C w) { v = cmulw<INV>(v, w); }
 
-template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twiddle(int tl, C* v, const C* __restrict__ tab) {
+template <int R, int N, int NS, bool INV, int VPT = 16>
+__device__ __forceinline__ void st_twiddle(int tl, C* v, const C* __restrict__ tab) {
   if constexpr (NS > 1) {
 #pragma unroll
-    for (int b = 0; b < st_nb<R>(); ++b) {
-      int j = tl + (N / 16) * b;
-      if (!st_has<R, N>(j)) { continue; }
+    for (int b = 0; b < st_nb<R, VPT>(); ++b) {
+      int j = tl + (N / VPT) * b;
+      if (!st_has<R, N, VPT>(j)) { continue; }
       int k = smod<NS>(j);
       C* x = v + b * R;
       if constexpr (R >= 8) {
@@ -276,16 +279,16 @@ template <int R, int N, int NS, bool INV> __device__ __forceinline__ void st_twi
   }
 }
 
-template <int R, bool INV> __device__ __forceinline__ void st_dft(C* v) {
+template <int R, bool INV, int VPT = 16> __device__ __forceinline__ void st_dft(C* v) {
 #pragma unroll
-  for (int b = 0; b < st_nb<R>(); ++b) { dftR<R, INV>(v + b * R); }
+  for (int b = 0; b < st_nb<R, VPT>(); ++b) { dftR<R, INV>(v + b * R); }
 }
 
-template <int R, int N, int NS, int PS> __device__ __forceinline__ void st_store(C* buf, int tl, const C* v) {
+template <int R, int N, int NS, int PS, int VPT = 16> __device__ __forceinline__ void st_store(C* buf, int tl, const C* v) {
 #pragma unroll
-  for (int b = 0; b < st_nb<R>(); ++b) {
-    int j = tl + (N / 16) * b;
-    if (!st_has<R, N>(j)) { continue; }
+  for (int b = 0; b < st_nb<R, VPT>(); ++b) {
+    int j = tl + (N / VPT) * b;
+    if (!st_has<R, N, VPT>(j)) { continue; }
     int base = sdiv<NS>(j) * NS * R + smod<NS>(j);
 #pragma unroll
     for (int r = 0; r < R; ++r) { buf[pad<PS>(base + r * NS)] = v[b * R + r]; }
@@ -297,13 +300,28 @@ template <int R, int N, int NS, int PS> __device__ __forceinline__ void st_store
 // "A order" runs the stages R1, M1, M2, RL; "B order" runs RL, M2, M1, R1.
 // n = 2^a or 5 * 2^a; the factor 5 becomes the M2 stage. r1f != 0 forces the
 // first radix (the split-precision column pass runs a 32-point first stage).
-constexpr int plan_r1(int n, int rl, int r1f = 0) { return r1f ? r1f : (n / rl >= 16 ? 16 : n / rl); }
-constexpr int plan_rest2(int n, int rl, int r1f = 0) { return n / rl / plan_r1(n, rl, r1f); }
-constexpr int plan_m1(int n, int rl, int r1f = 0) {
-  return plan_rest2(n, rl, r1f) % 5 == 0 ? plan_rest2(n, rl, r1f) / 5
-                                          : (plan_rest2(n, rl, r1f) >= 16 ? 16 : plan_rest2(n, rl, r1f));
+// vmax: the largest radix (the values per thread).
+constexpr int plan_r1(int n, int rl, int r1f = 0, int vmax = 16) {
+  return r1f ? r1f : (n / rl >= vmax ? vmax : n / rl);
 }
-constexpr int plan_m2(int n, int rl, int r1f = 0) { return plan_rest2(n, rl, r1f) / plan_m1(n, rl, r1f); }
+constexpr int plan_rest2(int n, int rl, int r1f = 0, int vmax = 16) { return n / rl / plan_r1(n, rl, r1f, vmax); }
+constexpr int plan_m1(int n, int rl, int r1f = 0, int vmax = 16) {
+  return plan_rest2(n, rl, r1f, vmax) % 5 == 0
+             ? plan_rest2(n, rl, r1f, vmax) / 5
+             : (plan_rest2(n, rl, r1f, vmax) >= vmax ? vmax : plan_rest2(n, rl, r1f, vmax));
+}
+constexpr int plan_m2(int n, int rl, int r1f = 0, int vmax = 16) {
+  return plan_rest2(n, rl, r1f, vmax) / plan_m1(n, rl, r1f, vmax);
+}
+
+// values per thread of the column pass for column length H: 8 (twice the threads at half the
+// registers) for power-of-two H <= 2048 when built with OWL_P2_VPT=8, else 16
+#ifndef OWL_P2_VPT
+#define OWL_P2_VPT 16
+#endif
+__host__ __device__ constexpr int p2_vpt(int H) {
+  return (OWL_P2_VPT == 8 && (H & (H - 1)) == 0 && H <= 2048) ? 8 : 16;
+}
 
 // Stage twiddle tables, one per stage with twiddles, each laid out [r][k]:
 // entry r * NS + k = w_(R NS)^(r k) (forward sign), so that a warp's threads
@@ -311,8 +329,8 @@ constexpr int plan_m2(int n, int rl, int r1f = 0) { return plan_rest2(n, rl, r1f
 struct TwOffsets {
   int aM1, aM2, aRL, bM2, bM1, bR1, total;
 };
-constexpr TwOffsets tw_offsets(int n, int rl, int r1f = 0) {
-  const int r1 = plan_r1(n, rl, r1f), m1 = plan_m1(n, rl, r1f), m2 = plan_m2(n, rl, r1f);
+constexpr TwOffsets tw_offsets(int n, int rl, int r1f = 0, int vmax = 16) {
+  const int r1 = plan_r1(n, rl, r1f, vmax), m1 = plan_m1(n, rl, r1f, vmax), m2 = plan_m2(n, rl, r1f, vmax);
   TwOffsets o{};
   o.aM1 = 0;
   o.aM2 = o.aM1 + (m1 > 1 ? m1 * r1 : 0);
@@ -324,15 +342,15 @@ constexpr TwOffsets tw_offsets(int n, int rl, int r1f = 0) {
   return o;
 }
 
-template <int N, int RL, int R1F = 0> struct Plan {
-  static constexpr int R1 = plan_r1(N, RL, R1F);
-  static constexpr int M1 = plan_m1(N, RL, R1F);
-  static constexpr int M2 = plan_m2(N, RL, R1F);
-  static constexpr TwOffsets TW = tw_offsets(N, RL, R1F);
+template <int N, int RL, int R1F = 0, int VPT = 16> struct Plan {
+  static constexpr int R1 = plan_r1(N, RL, R1F, VPT);
+  static constexpr int M1 = plan_m1(N, RL, R1F, VPT);
+  static constexpr int M2 = plan_m2(N, RL, R1F, VPT);
+  static constexpr TwOffsets TW = tw_offsets(N, RL, R1F, VPT);
   static_assert(R1 * M1 * M2 * RL == N, "plan");
-  static_assert(M2 >= 1 && M2 <= 16, "plan depth");
-  static_assert(M1 <= 16 && (16 % M1 == 0), "plan: first middle radix must divide 16");
-  static_assert(M2 == 5 || (16 % M2 == 0), "plan: second middle radix 5 or a divisor of 16");
+  static_assert(M2 >= 1 && M2 <= VPT, "plan depth");
+  static_assert(M1 <= VPT && (VPT % M1 == 0), "plan: first middle radix must divide the values per thread");
+  static_assert(M2 == 5 || (VPT % M2 == 0), "plan: second middle radix 5 or a divisor of the values per thread");
   static_assert(R1 >= 4, "first radix too small for conflict-free padding");
 };
 

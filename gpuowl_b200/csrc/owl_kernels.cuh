@@ -74,7 +74,8 @@ template <int W, int R> constexpr int p1_line_stride() {
   constexpr int ps = ilog2(16 / R) < ilog2(Plan<W, 16 / R>::R1) ? ilog2(16 / R) : ilog2(Plan<W, 16 / R>::R1);
   return W + (W >> ps) + 4;
 }
-template <int H> constexpr int p2_col_stride() { return H + (H >> 3) + 4; }
+// room for the smallest padding the column pass uses (one pad per RL = VPT/2 elements)
+template <int H, int VPT = 16> constexpr int p2_col_stride() { return H + (H >> ilog2(VPT / 2)) + 4; }
 enum : int { P2_SQUARE = 0, P2_FWD = 1, P2_MUL = 2 };
 enum : int { FL_MUL3 = 1, FL_LL = 2 };
 
@@ -511,14 +512,18 @@ __device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
   return cadd(s, p);
 }
 
-template <int H, int R, int MODE>
-__global__ void __launch_bounds__(H / 8, (H / 8 == 256) ? 2 : 1)
+// VPT: values per thread (16, or 8 for twice the threads at half the registers); the
+// cross-column last stage has radix RL = VPT/2 (A and B butterflies in one thread)
+template <int H, int R, int MODE, int VPT = 16>
+__global__ void __launch_bounds__(2 * H / VPT, ((2 * H / VPT == 256) || (VPT == 8 && 2 * H / VPT == 512)) ? 2 : 1)
     k_pass2(Args a, C* __restrict__ F, const C* __restrict__ Fb, C* __restrict__ Fq, int tslot) {
-  constexpr int T = H / 8;
-  constexpr int TC = H / 16;  // threads per column in the per-column stages
-  using P = Plan<H, 8>;
+  constexpr int RL = VPT / 2;
+  constexpr int T = H / RL;
+  constexpr int TC = H / VPT;  // threads per column in the per-column stages
+  using P = Plan<H, RL, 0, VPT>;
   constexpr int PS_R1 = ilog2(P::R1);
-  constexpr int CS = p2_col_stride<H>();
+  constexpr int PS_RL = ilog2(RL);
+  constexpr int CS = p2_col_stride<H, VPT>();
   OWL_DYN_SHARED(C, smem);
 
   const uint32_t W = a.W;
@@ -544,14 +549,14 @@ __global__ void __launch_bounds__(H / 8, (H / 8 == 256) ? 2 : 1)
   OWL_SHARED_ARR(C, s_step, 32);
   for (int i = t; i < 2 * P::R1; i += T) {
     const int cc = i / P::R1, rr = i % P::R1;
-    s_step[cc * 16 + rr] = bigtw(a, (cc ? kB : kA) * (uint32_t)(H / P::R1) * (uint32_t)rr);
+    s_step[cc * 16 + rr] = bigtw(a, (cc ? kB : kA) * (uint32_t)(H / P::R1) * (uint32_t)rr);  // R1 <= 16
   }
   __syncthreads();
 
-  C u[20];  // 16 values per thread; a radix-5 stage runs up to 4 butterflies
+  C u[VPT + 4];  // VPT values per thread; a radix-5 stage may run one butterfly more
   // ---- forward column DFT, first stage from HBM with the w_hN^(k1 j2) twiddle ----
 #pragma unroll
-  for (int b = 0; b < 16 / P::R1; ++b) {
+  for (int b = 0; b < VPT / P::R1; ++b) {
     int j = tcI + TC * b;
     const C base = bigtw(a, k1I * (uint32_t)j);
 #pragma unroll
@@ -561,137 +566,137 @@ __global__ void __launch_bounds__(H / 8, (H / 8 == 256) ? 2 : 1)
       u[b * P::R1 + r] = cmul(x, cmul(base, s_step[colI * 16 + r]));
     }
   }
-  st_dft<P::R1, false>(u);
-  st_store<P::R1, H, 1, PS_R1>(cbufI, tcI, u);
+  st_dft<P::R1, false, VPT>(u);
+  st_store<P::R1, H, 1, PS_R1, VPT>(cbufI, tcI, u);
   __syncthreads();
   constexpr int PS_AFTER_M1 = (P::M1 > 1) ? 4 : PS_R1;
   if constexpr (P::M1 > 1) {
-    st_load<P::M1, H, PS_R1>(cbuf, tc, u);
-    st_twiddle<P::M1, H, P::R1, false>(tc, u, a.twH + P::TW.aM1);
-    st_dft<P::M1, false>(u);
+    st_load<P::M1, H, PS_R1, VPT>(cbuf, tc, u);
+    st_twiddle<P::M1, H, P::R1, false, VPT>(tc, u, a.twH + P::TW.aM1);
+    st_dft<P::M1, false, VPT>(u);
     __syncthreads();
-    st_store<P::M1, H, P::R1, 4>(cbuf, tc, u);
+    st_store<P::M1, H, P::R1, 4, VPT>(cbuf, tc, u);
     __syncthreads();
   }
   constexpr int PS_AFTER_M2 = (P::M2 > 1) ? 4 : PS_AFTER_M1;
   if constexpr (P::M2 > 1) {
-    st_load<P::M2, H, PS_AFTER_M1>(cbuf, tc, u);
-    st_twiddle<P::M2, H, P::R1 * P::M1, false>(tc, u, a.twH + P::TW.aM2);
-    st_dft<P::M2, false>(u);
+    st_load<P::M2, H, PS_AFTER_M1, VPT>(cbuf, tc, u);
+    st_twiddle<P::M2, H, P::R1 * P::M1, false, VPT>(tc, u, a.twH + P::TW.aM2);
+    st_dft<P::M2, false, VPT>(u);
     __syncthreads();
-    st_store<P::M2, H, P::R1 * P::M1, 4>(cbuf, tc, u);
+    st_store<P::M2, H, P::R1 * P::M1, 4, VPT>(cbuf, tc, u);
     __syncthreads();
   }
-  // last forward stage (radix 8, NS = H/8 = T): A butterfly t, B butterfly T-1-t
+  // last forward stage (radix RL, NS = H/RL = T): A butterfly t, B butterfly T-1-t
   const int jB = T - 1 - t;
   C* bufA = smem;
   C* bufB = smem + CS;
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
+  for (int r = 0; r < RL; ++r) {
     u[r] = bufA[pad<PS_AFTER_M2>(t + r * T)];
-    u[8 + r] = bufB[pad<PS_AFTER_M2>(jB + r * T)];
+    u[RL + r] = bufB[pad<PS_AFTER_M2>(jB + r * T)];
   }
   if constexpr (T > 1) {
 #pragma unroll
-    for (int r = 1; r < 8; ++r) {
+    for (int r = 1; r < RL; ++r) {
       u[r] = cmul(u[r], __ldg(a.twH + P::TW.aRL + r * T + t));
-      u[8 + r] = cmul(u[8 + r], __ldg(a.twH + P::TW.aRL + r * T + jB));
+      u[RL + r] = cmul(u[RL + r], __ldg(a.twH + P::TW.aRL + r * T + jB));
     }
   }
-  dft8<false>(u);
-  dft8<false>(u + 8);
-  // now u[r] = ZA[t + T r], u[8 + r] = ZB[jB + T r]
+  dftR<RL, false>(u);
+  dftR<RL, false>(u + RL);
+  // now u[r] = ZA[t + T r], u[RL + r] = ZB[jB + T r]
 
   if constexpr (MODE == P2_FWD) {
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
+    for (int r = 0; r < RL; ++r) {
       uint32_t kA2 = t + T * r, kB2 = jB + T * r;
       Fq[faddr<R>(W, kA2, c, 0)] = u[r];
-      Fq[faddr<R>(W, kB2, c, 1)] = u[8 + r];
+      Fq[faddr<R>(W, kB2, c, 1)] = u[RL + r];
     }
     ts_end(a, tslot);
     return;
   } else {
     if (c != 0) {
-      // w_hN^(c + W k2) with k2 = t + (H/8) r is w_hN^c w_H^t w8^r
+      // w_hN^(c + W k2) with k2 = t + (H/RL) r is w_hN^c w_H^t w_RL^r
       const C base2 = cmul(bigtw(a, kA), __ldg(a.rootH + t));
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        uint32_t k2 = t + T * r;  // A index; partner is B[H-1-k2] = u[8 + 7 - r]
-        C t2 = mul_w8<false>(base2, r);
+      for (int r = 0; r < RL; ++r) {
+        uint32_t k2 = t + T * r;  // A index; partner is B[H-1-k2] = u[RL + RL-1 - r]
+        C t2 = mul_w8<false>(base2, r * (8 / RL));
         if constexpr (MODE == P2_SQUARE) {
-          pair_sq(u[r], u[15 - r], t2);
+          pair_sq(u[r], u[2 * RL - 1 - r], t2);
         } else {
           C cA = Fb[faddr<R>(W, k2, c, 0)];
           C cB = Fb[faddr<R>(W, H - 1 - k2, c, 1)];
-          pair_mul(u[r], u[15 - r], cA, cB, t2);
+          pair_mul(u[r], u[2 * RL - 1 - r], cA, cB, t2);
         }
       }
     } else {
       // columns 0 and W/2 pair with themselves: exchange through smem
       __syncthreads();
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
+      for (int r = 0; r < RL; ++r) {
         bufA[t + T * r] = u[r];
-        bufB[jB + T * r] = u[8 + r];
+        bufB[jB + T * r] = u[RL + r];
       }
       __syncthreads();
       const C baseA = __ldg(a.rootH + t);
       const C baseB = cmul(bigtw(a, W / 2), __ldg(a.rootH + jB));
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
+      for (int r = 0; r < RL; ++r) {
         uint32_t kA2 = t + T * r;
         uint32_t pA = (kA2 == 0) ? 0u : H - kA2;
         uint32_t kB2 = jB + T * r;
         uint32_t pB = H - 1 - kB2;
-        C t2A = mul_w8<false>(baseA, r);
-        C t2B = mul_w8<false>(baseB, r);
+        C t2A = mul_w8<false>(baseA, r * (8 / RL));
+        C t2B = mul_w8<false>(baseB, r * (8 / RL));
         if constexpr (MODE == P2_SQUARE) {
           u[r] = one_sq(u[r], bufA[pA], t2A);
-          u[8 + r] = one_sq(u[8 + r], bufB[pB], t2B);
+          u[RL + r] = one_sq(u[RL + r], bufB[pB], t2B);
         } else {
           C cA = Fb[faddr<R>(W, kA2, 0, 0)], dA = Fb[faddr<R>(W, pA, 0, 0)];
           C cB = Fb[faddr<R>(W, kB2, 0, 1)], dB = Fb[faddr<R>(W, pB, 0, 1)];
           u[r] = one_mul(u[r], bufA[pA], cA, dA, t2A);
-          u[8 + r] = one_mul(u[8 + r], bufB[pB], cB, dB, t2B);
+          u[RL + r] = one_mul(u[RL + r], bufB[pB], cB, dB, t2B);
         }
       }
     }
-    // ---- inverse column DFT: first stage (radix 8, NS = 1) from registers ----
-    dft8<true>(u);
-    dft8<true>(u + 8);
+    // ---- inverse column DFT: first stage (radix RL, NS = 1) from registers ----
+    dftR<RL, true>(u);
+    dftR<RL, true>(u + RL);
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      bufA[pad<3>(t * 8 + r)] = u[r];
-      bufB[pad<3>(jB * 8 + r)] = u[8 + r];
+    for (int r = 0; r < RL; ++r) {
+      bufA[pad<PS_RL>(t * RL + r)] = u[r];
+      bufB[pad<PS_RL>(jB * RL + r)] = u[RL + r];
     }
     __syncthreads();
-    constexpr int PS_I1 = (P::M2 > 1) ? 4 : 3;
+    constexpr int PS_I1 = (P::M2 > 1) ? 4 : PS_RL;
     if constexpr (P::M2 > 1) {
-      st_load<P::M2, H, 3>(cbuf, tc, u);
-      st_twiddle<P::M2, H, 8, true>(tc, u, a.twH + P::TW.bM2);
-      st_dft<P::M2, true>(u);
+      st_load<P::M2, H, PS_RL, VPT>(cbuf, tc, u);
+      st_twiddle<P::M2, H, RL, true, VPT>(tc, u, a.twH + P::TW.bM2);
+      st_dft<P::M2, true, VPT>(u);
       __syncthreads();
-      st_store<P::M2, H, 8, 4>(cbuf, tc, u);
+      st_store<P::M2, H, RL, 4, VPT>(cbuf, tc, u);
       __syncthreads();
     }
-    constexpr int NSi = 8 * P::M2;
+    constexpr int NSi = RL * P::M2;
     constexpr int PS_I2 = (P::M1 > 1) ? 4 : PS_I1;
     if constexpr (P::M1 > 1) {
-      st_load<P::M1, H, PS_I1>(cbuf, tc, u);
-      st_twiddle<P::M1, H, NSi, true>(tc, u, a.twH + P::TW.bM1);
-      st_dft<P::M1, true>(u);
+      st_load<P::M1, H, PS_I1, VPT>(cbuf, tc, u);
+      st_twiddle<P::M1, H, NSi, true, VPT>(tc, u, a.twH + P::TW.bM1);
+      st_dft<P::M1, true, VPT>(u);
       __syncthreads();
-      st_store<P::M1, H, NSi, 4>(cbuf, tc, u);
+      st_store<P::M1, H, NSi, 4, VPT>(cbuf, tc, u);
       __syncthreads();
     }
     constexpr int NSl = NSi * P::M1;  // == H / R1
-    st_load<P::R1, H, PS_I2>(cbufI, tcI, u);
-    st_twiddle<P::R1, H, NSl, true>(tcI, u, a.twH + P::TW.bR1);
-    st_dft<P::R1, true>(u);
+    st_load<P::R1, H, PS_I2, VPT>(cbufI, tcI, u);
+    st_twiddle<P::R1, H, NSl, true, VPT>(tcI, u, a.twH + P::TW.bR1);
+    st_dft<P::R1, true, VPT>(u);
 #pragma unroll
-    for (int b = 0; b < 16 / P::R1; ++b) {
+    for (int b = 0; b < VPT / P::R1; ++b) {
       int j = tcI + TC * b;
       const C base = bigtw(a, k1I * (uint32_t)j);
 #pragma unroll

@@ -59,9 +59,9 @@ inline uint32_t log2u(uint32_t x) {
 }
 
 // the stage twiddle tables of a length-n line FFT in the tw_offsets(n, rl) layout
-inline std::vector<HostC> stage_tables(uint32_t n, uint32_t rl, uint32_t r1f = 0) {
-  const TwOffsets o = tw_offsets((int)n, (int)rl, (int)r1f);
-  const uint32_t r1 = plan_r1(n, rl, r1f), m1 = plan_m1(n, rl, r1f), m2 = plan_m2(n, rl, r1f);
+inline std::vector<HostC> stage_tables(uint32_t n, uint32_t rl, uint32_t r1f = 0, uint32_t vmax = 16) {
+  const TwOffsets o = tw_offsets((int)n, (int)rl, (int)r1f, (int)vmax);
+  const uint32_t r1 = plan_r1(n, rl, r1f, vmax), m1 = plan_m1(n, rl, r1f, vmax), m2 = plan_m2(n, rl, r1f, vmax);
   std::vector<HostC> t(o.total);
   auto fill = [&](int off, uint32_t R, uint32_t NS) {
     for (uint32_t r = 0; r < R; ++r) {
@@ -164,7 +164,10 @@ inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
   const uint32_t N = t.N;
   t.loShift = (log2u(t.hN) + 1) / 2;
   t.twW = stage_tables(W, 16 / kLinesPerBlock);
-  t.twH = stage_tables(H, 8);
+  {
+    const uint32_t v = (uint32_t)p2_vpt((int)H);  // the column pass's values per thread
+    t.twH = stage_tables(H, v / 2, 0, v);
+  }
   t.rootH.resize(H);
   for (uint32_t i = 0; i < H; ++i) { t.rootH[i] = root(H, i); }
   uint32_t S = 1u << t.loShift;

@@ -105,10 +105,11 @@ template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int
   emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M>(a, F, words, slot, flags, -1); });
 }
 template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {
-  constexpr int T = H / 8;
-  size_t sm = 2 * (size_t)p2_col_stride<H>() * sizeof(C);
+  constexpr int V = p2_vpt(H);
+  constexpr int T = 2 * H / V;
+  size_t sm = 2 * (size_t)p2_col_stride<H, V>() * sizeof(C);
   Args a = p.a;
-  emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M>(a, F, Fb, Fq, -1); });
+  emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M, V>(a, F, Fb, Fq, -1); });
 }
 
 template <int M> void p2m_tc(EmuPlan& p, C* F, const C* Fb, C* Fq) {
