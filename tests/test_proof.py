@@ -111,3 +111,15 @@ def test_prp_proof_after_stop_and_resume(owl, tmp_path):
     r2 = owl.prp_run(E, W=64, H=64, block=500, save_dir=str(tmp_path), proof_power=4)
     assert r2["finished"] and r2["is_prime"] and r2["proof_power"] == 4
     assert owl.proof_verify(r2["proof_file"]) == (True, True)
+
+
+@pytest.mark.gpu
+def test_prp_of_m3021377_proves_prime_with_power_8(owl, tmp_path):
+    """A full PRP test of the Mersenne prime M3021377 (3.02 M iterations at the 256K FFT, Gerbicz
+    every 1,000) through the C++ driver, with a power-8 proof that then verifies."""
+    E = 3021377
+    r = owl.prp_run(E, save_dir=str(tmp_path), proof_power=8)
+    assert r["finished"] and r["is_prime"] and r["n_errors"] == 0
+    assert r["res64"] == 1                      # type-1 residue 3^(2^E) / 9 of a prime
+    assert r["proof_power"] == 8
+    assert owl.proof_verify(r["proof_file"]) == (True, True)
