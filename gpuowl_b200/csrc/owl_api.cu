@@ -119,7 +119,6 @@ struct owl_plan {
   const unsigned char* tcB = nullptr;
   const C* twHtc = nullptr;
   // device-side expand / compact: word staging (nWords + 1, zero padded), block carries, status
-  uint32_t p1Grid = 0;  // CTAs of the persistent carry-mode line pass (set on first launch)
   uint32_t* dwords = nullptr;
   uint32_t* packBlk = nullptr;
   owl::PackCtl* packCtl = nullptr;
@@ -163,33 +162,19 @@ void p2launch_tc(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts) {
   }
 }
 
-// CTAs of the persistent carry-mode line pass: as many as fit on the device at once (more would
-// only wait for a slot), at most one per line group
-template <int W> uint32_t p1_persistent_grid(owl_plan* p) {
-  constexpr int T = kR * W / 16;
-  const size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
-  int fused = 0, out = 0, sms = 0;
-  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fused, owl::k_pass1<W, kR, owl::P1_FUSED>, T, sm), "occupancy");
-  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&out, owl::k_pass1<W, kR, owl::P1_OUT>, T, sm), "occupancy");
-  ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device), "SM count");
-  const uint32_t n = (uint32_t)std::max(1, std::min(fused, out)) * (uint32_t)std::max(1, sms);
-  return std::min(n, p->H / (uint32_t)kR);
-}
-
 template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags, int ts) {
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
-  if (!p->p1Grid) { p->p1Grid = p1_persistent_grid<W>(p); }
-  const dim3 grid(p->H / kR), pgrid(p->p1Grid);
+  dim3 grid(p->H / kR);
   switch (mode) {
     case owl::P1_FUSED:
-      owl::k_pass1<W, kR, owl::P1_FUSED><<<pgrid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
+      owl::k_pass1<W, kR, owl::P1_FUSED><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
       break;
     case owl::P1_IN:
       owl::k_pass1<W, kR, owl::P1_IN><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
       break;
     default:
-      owl::k_pass1<W, kR, owl::P1_OUT><<<pgrid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
+      owl::k_pass1<W, kR, owl::P1_OUT><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
       break;
   }
 }

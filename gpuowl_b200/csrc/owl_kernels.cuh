@@ -30,8 +30,7 @@ struct Ctl {
   uint32_t ticket;    // line-group ticket for the carry chain (reset by the last taker)
   uint32_t error;     // DEVERR_* bits, sticky until the host clears them
   uint32_t npending;  // carries left over at the end of a thread's word chain (block exit only)
-  uint32_t done;      // CTAs of the current line pass that have left their group loop
-  uint32_t pad[28];
+  uint32_t pad[29];
 };
 
 enum : uint32_t { DEVERR_WAIT = 1u, DEVERR_PENDING = 2u };
@@ -164,22 +163,17 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   ts_begin(a, tslot);
   const int t = threadIdx.x;
   const uint32_t G = a.H / R;
-  // In the carry modes the CTAs are persistent: each takes line groups in ticket order, so that
-  // every lookback waits on a group that a running CTA holds. The next ticket is fetched once the
-  // current group's lookback wait is over (a CTA never holds a group it cannot start while it is
-  // blocked), and arrives while the rest of the group is worked on. The entry mode takes group
-  // blockIdx.x.
-  if constexpr (MODE != P1_IN) {
-    if (t == 0) { s_g = atomicAdd(&a.ctl->ticket, 1u); }
-    __syncthreads();
-  }
-  for (;;) {
   uint32_t g;
-  if constexpr (MODE == P1_IN) {
+  if (MODE == P1_IN) {
     g = blockIdx.x;
   } else {
+    if (t == 0) {
+      uint32_t tk = atomicAdd(&a.ctl->ticket, 1u);
+      if (tk == G - 1) { atomicExch(&a.ctl->ticket, 0u); }
+      s_g = tk;
+    }
+    __syncthreads();
     g = s_g;
-    if (g >= G) { break; }
   }
 
   const unsigned long long pol = l2_keep_policy();
@@ -359,7 +353,6 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
       }
     }
     __syncthreads();
-    if (t == 0) { s_g = atomicAdd(&a.ctl->ticket, 1u); }  // the next group
     // carry-in for line 0 of this group; column j1 of the last group wraps to
     // column j1 + 1 of group 0 (and the top word's carry to word 0)
     const uint32_t prevg = (g == 0) ? G - 1 : g - 1;
@@ -418,6 +411,8 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
           *reinterpret_cast<int2*>(words + 2 * ((size_t)a.H * j1 + j2)) = w2;
         }
       }
+      ts_end(a, tslot);
+      return;
     } else {
       p1_weight_line<W, R>(a, t, g, 0, dg[0], wrapmask, v);
       p1_fwd_first<W, R>(smem, t, v);
@@ -463,22 +458,8 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
         st_state(F + faddr<R>(W, g * R + l, c, s), u[b * P::R1 + r], pol);
       }
     }
+    ts_end(a, tslot);
   }
-  if constexpr (MODE == P1_IN) { break; }
-  __syncthreads();  // shared memory and s_g are reused by the next group
-  }  // group loop
-  if constexpr (MODE != P1_IN) {
-    // the last CTA out resets the ticket counter for the next line pass
-    if (t == 0) {
-      __threadfence();
-      if (atomicAdd(&a.ctl->done, 1u) == gridDim.x - 1) {
-        a.ctl->ticket = 0u;
-        a.ctl->done = 0u;
-        __threadfence();
-      }
-    }
-  }
-  ts_end(a, tslot);
 }
 
 // ---------------------------------------------------------------------------

@@ -161,7 +161,6 @@ __global__ void k_noalloc_tables(owl::Args a, uint32_t twWn, uint32_t twHn) {
     a.ctl->ticket = 0;
     a.ctl->error = 0;
     a.ctl->npending = 0;
-    a.ctl->done = 0;
   }
   for (uint32_t i = tid; i < kRoeSlots; i += nth) { a.roe[i] = 0.0f; }
 }
