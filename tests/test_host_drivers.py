@@ -26,8 +26,10 @@ def test_prp_of_composite(owl):
     assert r["finished"] and not r["is_prime"]
 
 
-@pytest.mark.parametrize("E", [86243, 132049])
+@pytest.mark.parametrize("E", [86243, 132049, 3021377])
 def test_ll_of_mersenne_prime(owl, E):
+    """LL to the end: the final value of a Mersenne prime is 0 (M3021377: 3.02 M iterations at
+    the 256K FFT)."""
     r = owl.ll_run(E)
     assert r["finished"] and r["is_prime"] and r["res64"] == 0
 
