@@ -177,6 +177,16 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   }
 
   const unsigned long long pol = l2_keep_policy();
+  // The inter-pass twiddle w_hN^(k1 j2) of this group's lines is applied here, on the way out
+  // (forward) and on the way in (inverse), not in the column pass: that pass is held by its FP64
+  // pipe, this one by latency. With k1 = j + (W/R1) r it is base(j) * step(line)^r; the steps of
+  // the R lines are tabulated per CTA (made visible by a barrier that the state loads overlap).
+  OWL_SHARED_ARR(C, s_tw, 2 * 16);
+  static_assert(R <= 2 && P::R1 <= 16, "line-pass twiddle table size");
+  for (int i = t; i < R * P::R1; i += T) {
+    const int ll = i / P::R1, rr = i % P::R1;
+    s_tw[ll * 16 + rr] = bigtw(a, (uint32_t)(W / P::R1) * (uint32_t)rr * (g * R + ll));
+  }
   // word classes of this thread's 32 words (fixed per shape, tabulated on the host)
   const uint2 wmask = __ldg(a.p1masks + (size_t)g * T + t);
   // per-line mapping for the inner stages
@@ -200,6 +210,14 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
           colpair(W, k1, c, s);
           u[b * P::R1 + r] = ld_state(F + faddr<R>(W, g * R + l, c, s), pol);
         }
+      }
+      __syncthreads();  // s_tw
+#pragma unroll
+      for (int b = 0; b < 16 / P::R1; ++b) {
+        const int j = tl + (W / 16) * b;
+        const C base = bigtw(a, (uint32_t)j * (g * R + l));
+#pragma unroll
+        for (int r = 0; r < P::R1; ++r) { u[b * P::R1 + r] = cmulc(u[b * P::R1 + r], cmul(base, s_tw[l * 16 + r])); }
       }
       st_dft<P::R1, true>(u);
       st_store<P::R1, W, 1, PS_R1>(line, tl, u);
@@ -451,11 +469,12 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
 #pragma unroll
     for (int b = 0; b < 16 / P::R1; ++b) {
       int j = tl + (W / 16) * b;
+      const C base = bigtw(a, (uint32_t)j * (g * R + l));
 #pragma unroll
       for (int r = 0; r < P::R1; ++r) {
         uint32_t k1 = j + r * (W / P::R1), c, s;
         colpair(W, k1, c, s);
-        st_state(F + faddr<R>(W, g * R + l, c, s), u[b * P::R1 + r], pol);
+        st_state(F + faddr<R>(W, g * R + l, c, s), cmul(u[b * P::R1 + r], cmul(base, s_tw[l * 16 + r])), pol);
       }
     }
     ts_end(a, tslot);
@@ -540,30 +559,19 @@ __global__ void __launch_bounds__(2 * H / VPT, ((2 * H / VPT == 256) || (VPT == 
   // (both columns of R lines of one line group) of the tile layout
   const int colI = (t >> 1) & 1;
   const int tcI = ((t >> 2) << 1) | (t & 1);
-  const uint32_t k1I = colI ? kB : kA;
   C* cbufI = smem + colI * CS;
 
   const unsigned long long pol = l2_keep_policy();
-  // w_hN^(k1 j2) for j2 = j + (H/R1) r is base(j) * step^r: base per butterfly,
-  // step^r per column in shared memory (one rounding more than a table value)
-  OWL_SHARED_ARR(C, s_step, 32);
-  for (int i = t; i < 2 * P::R1; i += T) {
-    const int cc = i / P::R1, rr = i % P::R1;
-    s_step[cc * 16 + rr] = bigtw(a, (cc ? kB : kA) * (uint32_t)(H / P::R1) * (uint32_t)rr);  // R1 <= 16
-  }
-  __syncthreads();
 
   C u[VPT + 4];  // VPT values per thread; a radix-5 stage may run one butterfly more
-  // ---- forward column DFT, first stage from HBM with the w_hN^(k1 j2) twiddle ----
+  // ---- forward column DFT, first stage from HBM (the line pass applied the w_hN^(k1 j2) twiddle) ----
 #pragma unroll
   for (int b = 0; b < VPT / P::R1; ++b) {
     int j = tcI + TC * b;
-    const C base = bigtw(a, k1I * (uint32_t)j);
 #pragma unroll
     for (int r = 0; r < P::R1; ++r) {
       uint32_t j2 = j + r * (H / P::R1);
-      C x = ld_state(F + faddr<R>(W, j2, c, colI), pol);
-      u[b * P::R1 + r] = cmul(x, cmul(base, s_step[colI * 16 + r]));
+      u[b * P::R1 + r] = ld_state(F + faddr<R>(W, j2, c, colI), pol);
     }
   }
   st_dft<P::R1, false, VPT>(u);
@@ -698,11 +706,10 @@ __global__ void __launch_bounds__(2 * H / VPT, ((2 * H / VPT == 256) || (VPT == 
 #pragma unroll
     for (int b = 0; b < VPT / P::R1; ++b) {
       int j = tcI + TC * b;
-      const C base = bigtw(a, k1I * (uint32_t)j);
 #pragma unroll
       for (int r = 0; r < P::R1; ++r) {
         uint32_t j2 = j + r * (H / P::R1);
-        st_state(F + faddr<R>(W, j2, c, colI), cmulc(u[b * P::R1 + r], cmul(base, s_step[colI * 16 + r])), pol);
+        st_state(F + faddr<R>(W, j2, c, colI), u[b * P::R1 + r], pol);
       }
     }
     ts_end(a, tslot);

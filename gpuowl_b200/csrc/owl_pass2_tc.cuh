@@ -238,12 +238,6 @@ __global__ void __launch_bounds__(kTcH / 8, 2)
     uint4* dst = reinterpret_cast<uint4*>(sB);
     for (int i = t; i < kTcBBytes / 16; i += T) { dst[i] = __ldg(src + i); }
   }
-  // w_hN^(k1 j2) for j2 = j + 64 r is base(j) * step^r, step^r per column here
-  OWL_SHARED_ARR(C, s_step, 2 * kTcR1);
-  for (int i = t; i < 2 * kTcR1; i += T) {
-    const int cc = i / kTcR1, rr = i % kTcR1;
-    s_step[i] = bigtw(a, (cc ? kB : kA) * (uint32_t)(H / kTcR1) * (uint32_t)rr);
-  }
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
@@ -254,16 +248,12 @@ __global__ void __launch_bounds__(kTcH / 8, 2)
 
   C u[16];
   C y[16];
-  // ---- forward: inputs from HBM with the w_hN^(k1 j2) twiddle ----
-  {
-    const uint32_t k1 = gcol ? kB : kA;
-    const C base = bigtw(a, k1 * (uint32_t)gj);
+  // ---- forward: inputs from HBM (the line pass applied the w_hN^(k1 j2) twiddle) ----
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int r = 16 * ghh + i;
-      const uint32_t j2 = (uint32_t)(gj + 64 * r);
-      u[i] = cmul(ld_state(F + faddr<R>(W, j2, c, gcol), pol), cmul(base, s_step[gcol * kTcR1 + r]));
-    }
+  for (int i = 0; i < 16; ++i) {
+    const int r = 16 * ghh + i;
+    const uint32_t j2 = (uint32_t)(gj + 64 * r);
+    u[i] = ld_state(F + faddr<R>(W, j2, c, gcol), pol);
   }
   ok &= tc_dft32<false>(a, sA, sExp, sBar, aBase, bBase, taddr, phase, grow, ghh, u, y);
   {
@@ -375,15 +365,11 @@ __global__ void __launch_bounds__(kTcH / 8, 2)
       }
     }
     ok &= tc_dft32<true>(a, sA, sExp, sBar, aBase, bBase, taddr, phase, grow, ghh, u, y);
-    {
-      const uint32_t k1 = dcol ? kB : kA;
-      const C base = bigtw(a, k1 * (uint32_t)dj);
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const int mm = (k < 8) ? dm0 + k : 16 + dm0 + (k - 8);
-        const uint32_t j2 = (uint32_t)(dj + 64 * mm);
-        st_state(F + faddr<R>(W, j2, c, dcol), cmulc(y[k], cmul(base, s_step[dcol * kTcR1 + mm])), pol);
-      }
+    for (int k = 0; k < 16; ++k) {
+      const int mm = (k < 8) ? dm0 + k : 16 + dm0 + (k - 8);
+      const uint32_t j2 = (uint32_t)(dj + 64 * mm);
+      st_state(F + faddr<R>(W, j2, c, dcol), y[k], pol);
     }
   }
   if (!ok && threadIdx.x == 0) { atomicOr(&a.ctl->error, DEVERR_WAIT); }
