@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   static_assert(R <= 2 && P::R1 <= 16, "line-pass twiddle table size");
   for (int i = t; i < R * P::R1; i += T) {
     const int ll = i / P::R1, rr = i % P::R1;
-    s_tw[ll * 16 + rr] = bigtw(a, (uint32_t)(W / P::R1) * (uint32_t)rr * (g * R + ll));
+    s_tw[rr * R + ll] = bigtw(a, (uint32_t)(W / P::R1) * (uint32_t)rr * (g * R + ll));  // lines adjacent
   }
   // word classes of this thread's 32 words (fixed per shape, tabulated on the host)
   const uint2 wmask = __ldg(a.p1masks + (size_t)g * T + t);
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
         const int j = tl + (W / 16) * b;
         const C base = bigtw(a, (uint32_t)j * (g * R + l));
 #pragma unroll
-        for (int r = 0; r < P::R1; ++r) { u[b * P::R1 + r] = cmulc(u[b * P::R1 + r], cmul(base, s_tw[l * 16 + r])); }
+        for (int r = 0; r < P::R1; ++r) { u[b * P::R1 + r] = cmulc(u[b * P::R1 + r], cmul(base, s_tw[r * R + l])); }
       }
       st_dft<P::R1, true>(u);
       st_store<P::R1, W, 1, PS_R1>(line, tl, u);
@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
       for (int r = 0; r < P::R1; ++r) {
         uint32_t k1 = j + r * (W / P::R1), c, s;
         colpair(W, k1, c, s);
-        st_state(F + faddr<R>(W, g * R + l, c, s), cmul(u[b * P::R1 + r], cmul(base, s_tw[l * 16 + r])), pol);
+        st_state(F + faddr<R>(W, g * R + l, c, s), cmul(u[b * P::R1 + r], cmul(base, s_tw[r * R + l])), pol);
       }
     }
     ts_end(a, tslot);
