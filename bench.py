@@ -292,6 +292,11 @@ def run_ours(args, rank, world, local):
             pin_in = torch.empty(plan.nwords, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
             pin_out = torch.empty(plan.nwords, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
             plan.readOut(data, out=pin_in)
+            # one untimed pass first: squareLoop's graph for this buffer pair is captured on first use
+            plan.writeIn(data, pin_in)
+            plan.modMul(check, data)
+            plan.squareLoop(data, data, B)
+            plan.readOut(data, out=pin_in)
             barrier()
             for _ in range(max(2, steps // 2)):
                 torch.cuda.synchronize()

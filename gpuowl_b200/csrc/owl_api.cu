@@ -146,55 +146,58 @@ template <int M> void setp2tcattr() {
      "cudaFuncSetAttribute(pass2 split)");
 }
 
-void p2launch_tc(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts) {
-  dim3 grid(p->W / 2);
-  constexpr int T = owl::kTcH / 8;
-  switch (mode) {
-    case owl::P2_SQUARE:
-      owl::k_pass2_tc<kR, owl::P2_SQUARE><<<grid, T, owl::kTcSmem, p->stream>>>(p->args, p->tcB, p->twHtc, F, Fb, Fq, ts);
-      break;
-    case owl::P2_FWD:
-      owl::k_pass2_tc<kR, owl::P2_FWD><<<grid, T, owl::kTcSmem, p->stream>>>(p->args, p->tcB, p->twHtc, F, Fb, Fq, ts);
-      break;
-    default:
-      owl::k_pass2_tc<kR, owl::P2_MUL><<<grid, T, owl::kTcSmem, p->stream>>>(p->args, p->tcB, p->twHtc, F, Fb, Fq, ts);
-      break;
+// Launches a pass kernel on the plan's stream. With `pdl` it is a programmatic dependent of the
+// kernel before it (the pass kernels begin with griddep_wait()): its CTAs may be scheduled on SMs
+// that the previous pass's last CTAs leave free, which hides the launch gap between the passes.
+template <typename... KArgs, typename... Args>
+void launch_pass(owl_plan* p, bool pdl, void (*kernel)(KArgs...), dim3 grid, int threads, size_t smem,
+                 Args... args) {
+  if (!pdl) {
+    kernel<<<grid, threads, smem, p->stream>>>(args...);
+    return;
   }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = p->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ck(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...), "cudaLaunchKernelEx");
 }
 
-template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags, int ts) {
+void p2launch_tc(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
+  dim3 grid(p->W / 2);
+  constexpr int T = owl::kTcH / 8;
+  auto k = (mode == owl::P2_SQUARE) ? owl::k_pass2_tc<kR, owl::P2_SQUARE>
+           : (mode == owl::P2_FWD)  ? owl::k_pass2_tc<kR, owl::P2_FWD>
+                                    : owl::k_pass2_tc<kR, owl::P2_MUL>;
+  launch_pass(p, pdl, k, grid, T, owl::kTcSmem, p->args, (const unsigned char*)p->tcB, (const C*)p->twHtc, F, Fb, Fq,
+              ts);
+}
+
+template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags, int ts, bool pdl) {
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
   dim3 grid(p->H / kR);
-  switch (mode) {
-    case owl::P1_FUSED:
-      owl::k_pass1<W, kR, owl::P1_FUSED><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
-      break;
-    case owl::P1_IN:
-      owl::k_pass1<W, kR, owl::P1_IN><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
-      break;
-    default:
-      owl::k_pass1<W, kR, owl::P1_OUT><<<grid, T, sm, p->stream>>>(p->args, F, words, roeSlot, flags, ts);
-      break;
-  }
+  auto k = (mode == owl::P1_FUSED) ? owl::k_pass1<W, kR, owl::P1_FUSED>
+           : (mode == owl::P1_IN)  ? owl::k_pass1<W, kR, owl::P1_IN>
+                                   : owl::k_pass1<W, kR, owl::P1_OUT>;
+  launch_pass(p, pdl, k, grid, T, sm, p->args, F, words, roeSlot, flags, ts);
 }
 
-template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts) {
+template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
   constexpr int V = owl::p2_vpt(H);
   constexpr int T = 2 * H / V;
   size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
   dim3 grid(p->W / 2);
-  switch (mode) {
-    case owl::P2_SQUARE:
-      owl::k_pass2<H, kR, owl::P2_SQUARE, V><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
-      break;
-    case owl::P2_FWD:
-      owl::k_pass2<H, kR, owl::P2_FWD, V><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
-      break;
-    default:
-      owl::k_pass2<H, kR, owl::P2_MUL, V><<<grid, T, sm, p->stream>>>(p->args, F, Fb, Fq, ts);
-      break;
-  }
+  auto k = (mode == owl::P2_SQUARE) ? owl::k_pass2<H, kR, owl::P2_SQUARE, V>
+           : (mode == owl::P2_FWD)  ? owl::k_pass2<H, kR, owl::P2_FWD, V>
+                                    : owl::k_pass2<H, kR, owl::P2_MUL, V>;
+  launch_pass(p, pdl, k, grid, T, sm, p->args, F, Fb, Fq, ts);
 }
 
 #define OWL_FOR_SIZES(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
@@ -233,7 +236,8 @@ void set_attrs(uint32_t W, uint32_t H) {
   }
 }
 
-void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot = -1, int ts = -1) {
+void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot = -1, int ts = -1,
+           bool pdl = false) {
   int slot = -1;
   if (mode != owl::P1_IN) {
     if (fixedSlot >= 0) {
@@ -247,7 +251,7 @@ void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot
   switch (p->W) {
 #define CASE_W(n)                                \
   case n:                                        \
-    p1launch<n>(p, mode, F, words, slot, flags, ts); \
+    p1launch<n>(p, mode, F, words, slot, flags, ts, pdl); \
     break;
     OWL_FOR_SIZES(CASE_W)
 #undef CASE_W
@@ -257,16 +261,16 @@ void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot
   ck(cudaGetLastError(), "pass1 launch");
 }
 
-void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts = -1) {
+void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts = -1, bool pdl = false) {
   if (p->split) {
-    p2launch_tc(p, mode, F, Fb, Fq, ts);
+    p2launch_tc(p, mode, F, Fb, Fq, ts, pdl);
     ck(cudaGetLastError(), "pass2 split launch");
     return;
   }
   switch (p->H) {
 #define CASE_H(n)                       \
   case n:                               \
-    p2launch<n>(p, mode, F, Fb, Fq, ts); \
+    p2launch<n>(p, mode, F, Fb, Fq, ts, pdl); \
     break;
     OWL_FOR_H_SIZES(CASE_H)
 #undef CASE_H
@@ -277,8 +281,8 @@ void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts = -1) {
 }
 
 // the block-exit line pass, then the (normally empty) queue of leftover carries
-void pass1_out(owl_plan* p, int32_t* words, int flags, int fixedSlot = -1, int ts = -1) {
-  pass1(p, owl::P1_OUT, p->F1, words, flags, fixedSlot, ts);
+void pass1_out(owl_plan* p, int32_t* words, int flags, int fixedSlot = -1, int ts = -1, bool pdl = false) {
+  pass1(p, owl::P1_OUT, p->F1, words, flags, fixedSlot, ts, pdl);
   owl::k_carry_fixup<<<1, 32, 0, p->stream>>>(p->args, words);
   ck(cudaGetLastError(), "fixup launch");
 }
@@ -300,13 +304,16 @@ void enqueue_square(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, ui
     ck(cudaMemsetAsync(p->args.tsStart, 0xff, cnt * sizeof(unsigned long long), p->stream), "memset ts");
     ck(cudaMemsetAsync(p->args.tsEnd, 0, cnt * sizeof(unsigned long long), p->stream), "memset ts");
   }
+  // the passes after the entry pass are programmatic dependents of the pass before them, except
+  // the line pass after the split-precision column pass (8 us slower per iteration at 8M that way)
+  const bool pdl = !p->split;
   pass1(p, owl::P1_IN, p->F1, const_cast<int32_t*>(in), 0, -1, ts());
   for (uint32_t k = 0; k < n; ++k) {
-    pass2(p, owl::P2_SQUARE, p->F1, nullptr, nullptr, ts());
+    pass2(p, owl::P2_SQUARE, p->F1, nullptr, nullptr, ts(), true);
     if (k + 1 < n) {
-      pass1(p, owl::P1_FUSED, p->F1, nullptr, ll, (int)k, ts());
+      pass1(p, owl::P1_FUSED, p->F1, nullptr, ll, (int)k, ts(), pdl);
     } else {
-      pass1_out(p, out, ll | mul3, (int)k, ts());
+      pass1_out(p, out, ll | mul3, (int)k, ts(), pdl);
     }
   }
 }

@@ -31,6 +31,14 @@ __device__ __forceinline__ unsigned long long gtimer() {
 // __nanosleep between polls measured 1.4 us slower per line pass at 8M
 __device__ __forceinline__ void spin_pause() {}
 
+// Programmatic dependent launch. A kernel launched with programmatic stream serialization may be
+// scheduled while the previous kernel on its stream is still finishing: griddep_wait() returns once
+// that kernel has completed and its memory operations are visible (at once for a normal launch).
+// griddep_launch() allows the next such kernel to be scheduled once every CTA of this one has
+// called it (or exited).
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // The FFT state is streamed through L1 without allocating (so that the twiddle
 // and weight tables stay resident) and kept in L2 with evict-last priority: at
 // 8M words the 64 MiB state fits in the 126 MB L2 between the two passes.

@@ -160,6 +160,10 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   OWL_SHARED(uint32_t, s_g);
   OWL_SHARED_ARR(float, s_roe, 32);
 
+  // launched as a programmatic dependent of the column pass: nothing (ticket included) is touched
+  // before that pass has completed
+  griddep_wait();
+  griddep_launch();
   ts_begin(a, tslot);
   const int t = threadIdx.x;
   const uint32_t G = a.H / R;
@@ -332,14 +336,15 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
     for (int ll = 0; ll < R; ++ll) { p1_fwd_first<W, R>(smem + ll * LS, t, v + ll * RL); }
     __syncthreads();
   } else {
-    // publish this group's carry row
-    __threadfence();
+    // publish this group's carry row: the barrier below orders every thread's shuttle stores
+    // before thread 0's fence and release of the flag (one fence per CTA, as in a grid barrier)
     constexpr unsigned WMASK = (T >= 32) ? 0xffffffffu : ((1u << T) - 1u);
 #pragma unroll
     for (int o = (T >= 32 ? 16 : T / 2); o > 0; o >>= 1) { roe = fmaxf(roe, __shfl_xor_sync(WMASK, roe, o)); }
     if ((t & 31) == 0) { s_roe[t >> 5] = roe; }
-    __syncthreads();  // carries fenced; the inverse DFT's shared-memory reads are done
+    __syncthreads();  // carries stored; the inverse DFT's shared-memory reads are done
     if (t == 0) {
+      __threadfence();
       st_release(a.flags + g, 1u);
       float m = 0.0f;
       for (int i = 0; i < (T + 31) / 32; ++i) { m = fmaxf(m, s_roe[i]); }
@@ -547,6 +552,8 @@ __global__ void __launch_bounds__(2 * H / VPT, ((2 * H / VPT == 256) || (VPT == 
 
   const uint32_t W = a.W;
   const uint32_t c = blockIdx.x;
+  griddep_wait();
+  griddep_launch();
   ts_begin(a, tslot);
   const int t = threadIdx.x;
   const int col = t / TC;

@@ -212,6 +212,8 @@ __global__ void __launch_bounds__(kTcH / 8, 2)
 
   const uint32_t W = a.W;
   const uint32_t c = blockIdx.x;
+  griddep_wait();
+  griddep_launch();
   ts_begin(a, tslot);
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int col = t / TC;

@@ -176,6 +176,8 @@ inline unsigned long long gtimer() {
       .count();
 }
 inline void spin_pause() { std::this_thread::yield(); }
+inline void griddep_wait() {}
+inline void griddep_launch() {}
 inline unsigned long long l2_keep_policy() { return 0; }
 inline double2 ld_state(const double2* p, unsigned long long) { return *p; }
 inline void st_state(double2* p, double2 v, unsigned long long) { *p = v; }
