@@ -37,6 +37,10 @@ enum : uint32_t { DEVERR_WAIT = 1u, DEVERR_PENDING = 2u };
 constexpr uint32_t kPendingCap = 1024;
 
 struct Args {
+  // the carry's two FP64 constants first, as a 16-byte-aligned pair (with them at offset 184 the
+  // 8M line pass spilled a register and ran 1.8 us slower)
+  double scaleLo;      // 2^bitsLo
+  double iscaleLo;     // 2^-bitsLo
   const C* twW;    // stage tables of the width FFT (tw_offsets(W, 16/R) layout)
   const C* twH;    // stage tables of the height FFT (tw_offsets(H, 8) layout)
   const C* rootH;  // w_H^i, i < H
@@ -60,8 +64,6 @@ struct Args {
   uint32_t E, N, W, H, hN;
   uint32_t bitsLo;     // E / N
   uint32_t eModN;      // E % N (a word is big iff its extra < E % N)
-  double scaleLo;      // 2^bitsLo
-  double iscaleLo;     // 2^-bitsLo
   uint32_t loShift;
   unsigned long long timeoutNs;
 };
@@ -181,6 +183,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   }
 
   const unsigned long long pol = l2_keep_policy();
+  const C* __restrict__ twW = a.twW;  // the width stage tables, read-only for the whole pass
   // The inter-pass twiddle w_hN^(k1 j2) of this group's lines is applied here, on the way out
   // (forward) and on the way in (inverse), not in the column pass: that pass is held by its FP64
   // pipe, this one by latency. With k1 = j + (W/R1) r it is base(j) * step(line)^r; the steps of
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
       constexpr int PS_AFTER_M1 = (P::M1 > 1) ? 4 : PS_R1;
       if constexpr (P::M1 > 1) {
         st_load<P::M1, W, PS_R1>(line, tl, u);
-        st_twiddle<P::M1, W, NS2, true>(tl, u, a.twW + P::TW.aM1);
+        st_twiddle<P::M1, W, NS2, true>(tl, u, twW + P::TW.aM1);
         st_dft<P::M1, true>(u);
         __syncthreads();
         st_store<P::M1, W, NS2, 4>(line, tl, u);
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
       constexpr int PS_AFTER_M2 = (P::M2 > 1) ? 4 : PS_AFTER_M1;
       if constexpr (P::M2 > 1) {
         st_load<P::M2, W, PS_AFTER_M1>(line, tl, u);
-        st_twiddle<P::M2, W, NS3, true>(tl, u, a.twW + P::TW.aM2);
+        st_twiddle<P::M2, W, NS3, true>(tl, u, twW + P::TW.aM2);
         st_dft<P::M2, true>(u);
         __syncthreads();
         st_store<P::M2, W, NS3, 4>(line, tl, u);
@@ -255,7 +258,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
         for (int r = 0; r < RL; ++r) { v[ll * RL + r] = ln[pad<PS_AFTER_M2>(t + r * NSL)]; }
         if constexpr (NSL > 1) {
 #pragma unroll
-          for (int r = 1; r < RL; ++r) { v[ll * RL + r] = cmulw<true>(v[ll * RL + r], __ldg(a.twW + P::TW.aRL + r * NSL + t)); }
+          for (int r = 1; r < RL; ++r) { v[ll * RL + r] = cmulw<true>(v[ll * RL + r], __ldg(twW + P::TW.aRL + r * NSL + t)); }
         }
         dftR<RL, true>(v + ll * RL);
       }
@@ -450,7 +453,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
     constexpr int PS_A = (P::M2 > 1) ? 4 : PS_RL;
     if constexpr (P::M2 > 1) {
       st_load<P::M2, W, PS_RL>(line, tl, u);
-      st_twiddle<P::M2, W, NSa, false>(tl, u, a.twW + P::TW.bM2);
+      st_twiddle<P::M2, W, NSa, false>(tl, u, twW + P::TW.bM2);
       st_dft<P::M2, false>(u);
       __syncthreads();
       st_store<P::M2, W, NSa, 4>(line, tl, u);
@@ -460,7 +463,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
     constexpr int PS_B = (P::M1 > 1) ? 4 : PS_A;
     if constexpr (P::M1 > 1) {
       st_load<P::M1, W, PS_A>(line, tl, u);
-      st_twiddle<P::M1, W, NSb, false>(tl, u, a.twW + P::TW.bM1);
+      st_twiddle<P::M1, W, NSb, false>(tl, u, twW + P::TW.bM1);
       st_dft<P::M1, false>(u);
       __syncthreads();
       st_store<P::M1, W, NSb, 4>(line, tl, u);
@@ -468,7 +471,7 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
     }
     constexpr int NSc = NSb * P::M1;  // == W / R1
     st_load<P::R1, W, PS_B>(line, tl, u);
-    st_twiddle<P::R1, W, NSc, false>(tl, u, a.twW + P::TW.bR1);
+    st_twiddle<P::R1, W, NSc, false>(tl, u, twW + P::TW.bR1);
     st_dft<P::R1, false>(u);
     // outputs k1 = j + r (W/R1) straight to HBM
 #pragma unroll
@@ -537,9 +540,14 @@ __device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
 }
 
 // VPT: values per thread (16, or 8 for twice the threads at half the registers); the
-// cross-column last stage has radix RL = VPT/2 (A and B butterflies in one thread)
+// cross-column last stage has radix RL = VPT/2 (A and B butterflies in one thread).
+// Occupancy hint: 2 CTAs per SM for the 256-thread (and 512-thread VPT 8) columns; 3 for the
+// 160-thread H = 1280 columns, which otherwise take 243 registers and run one 5-warp CTA per SM
+// (5M: 45.5 -> 32.6 us per column pass with a few spilled registers). The 320-thread H = 2560
+// columns stay at one CTA: two would cap them at 102 registers.
 template <int H, int R, int MODE, int VPT = 16>
-__global__ void __launch_bounds__(2 * H / VPT, ((2 * H / VPT == 256) || (VPT == 8 && 2 * H / VPT == 512)) ? 2 : 1)
+__global__ void __launch_bounds__(2 * H / VPT,
+                                  ((2 * H / VPT == 256) || (VPT == 8 && 2 * H / VPT == 512)) ? 2 : (H == 1280 ? 3 : 1))
     k_pass2(Args a, C* __restrict__ F, const C* __restrict__ Fb, C* __restrict__ Fq, int tslot) {
   constexpr int RL = VPT / 2;
   constexpr int T = H / RL;
