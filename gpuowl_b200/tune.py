@@ -88,6 +88,37 @@ def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True, five=False
     return rows
 
 
+def profile_shapes(shapes, iters, bpw=16.0, device=0):
+    """Per-kernel device time of `iters` squarings on each W x H shape (the -time profile per shape):
+    E is the first odd number above N * bpw, the residue random; one untimed block first."""
+    import numpy as np
+    import gpuowl_b200 as owl
+    from gpuowl_b200 import build
+    build.build()
+    rows = []
+    for (W, H) in shapes:
+        N = 2 * W * H
+        E = next_odd_exponent(N * bpw)
+        with owl.Plan(E, device=device, W=W, H=H) as p:
+            b = p.alloc()
+            rng = np.random.default_rng(N)
+            w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
+            if E % 32:
+                w[-1] &= (1 << (E % 32)) - 1
+            p.writeIn(b, w)
+            p.profile_square(b, iters)
+            p.readROE()
+            prof = p.profile_square(b, iters)
+            roe = float(p.readROE().max())
+        us2 = 1e3 * prof["pass2"][0] / prof["pass2"][1]
+        us1 = 1e3 * prof["pass1"][0] / prof["pass1"][1]
+        total = 1e3 * (prof["pass2"][0] + prof["pass1"][0] + prof["edge"][0]) / iters
+        rows.append((N, W, H, total, us2, us1, roe))
+        print("N=%-9d %-14s %8.2f us/iter  column pass %7.2f us  line pass %7.2f us  max ROE %.4f"
+              % (N, spec(W, H), total, us2, us1, roe), flush=True)
+    return rows
+
+
 def roe_at(N, W, H, bpw, iters, device=0):
     """Max round-off of `iters` squarings of a random residue at E = N * bpw (odd) on W x H."""
     import numpy as np
@@ -167,7 +198,11 @@ def main():
     ap.add_argument("--five", action="store_true", help="also the 5 * 2^k FFT lengths")
     ap.add_argument("--bpw-scan", metavar="TUNE_JSON", help="measure the max bits/word of the shapes in TUNE_JSON")
     ap.add_argument("--roe-limit", type=float, default=0.3)
+    ap.add_argument("--shapes", metavar="WxH,...", help="per-pass times of these shapes (at 16 bits/word)")
     a = ap.parse_args()
+    if a.shapes:
+        profile_shapes([tuple(int(v) for v in s.split("x")) for s in a.shapes.split(",")], a.iters)
+        return
     if a.bpw_scan:
         with open(a.bpw_scan) as f:
             t = json.load(f)
