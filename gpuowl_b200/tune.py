@@ -88,9 +88,10 @@ def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True, five=False
     return rows
 
 
-def profile_shapes(shapes, iters, bpw=16.0, device=0):
+def profile_shapes(shapes, iters, bpw=16.0, device=0, split=False):
     """Per-kernel device time of `iters` squarings on each W x H shape (the -time profile per shape):
-    E is the first odd number above N * bpw, the residue random; one untimed block first."""
+    E is the first odd number above N * bpw, the residue random; one untimed block first. With
+    `split` the column pass runs in the split-precision form (H = 2048 only)."""
     import numpy as np
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
@@ -99,7 +100,7 @@ def profile_shapes(shapes, iters, bpw=16.0, device=0):
     for (W, H) in shapes:
         N = 2 * W * H
         E = next_odd_exponent(N * bpw)
-        with owl.Plan(E, device=device, W=W, H=H) as p:
+        with owl.Plan(E, device=device, W=W, H=H, split=split) as p:
             b = p.alloc()
             rng = np.random.default_rng(N)
             w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
@@ -199,9 +200,11 @@ def main():
     ap.add_argument("--bpw-scan", metavar="TUNE_JSON", help="measure the max bits/word of the shapes in TUNE_JSON")
     ap.add_argument("--roe-limit", type=float, default=0.3)
     ap.add_argument("--shapes", metavar="WxH,...", help="per-pass times of these shapes (at 16 bits/word)")
+    ap.add_argument("--split", action="store_true", help="with --shapes: the split-precision column pass")
     a = ap.parse_args()
     if a.shapes:
-        profile_shapes([tuple(int(v) for v in s.split("x")) for s in a.shapes.split(",")], a.iters)
+        profile_shapes([tuple(int(v) for v in s.split("x")) for s in a.shapes.split(",")], a.iters,
+                       split=a.split)
         return
     if a.bpw_scan:
         with open(a.bpw_scan) as f:
