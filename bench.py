@@ -47,8 +47,9 @@ def parse():
     ap.add_argument("--block", type=int, default=BLOCK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tensor-core) form")
-    ap.add_argument("--workload", default="prp8m", choices=["prp8m", "batch64"],
-                    help="prp8m: the headline line; batch64: 64 uneven exponents in one graph per block")
+    ap.add_argument("--workload", default="prp8m", choices=["prp8m", "batch64", "prp20m"],
+                    help="prp8m: the headline line; batch64: 64 uneven exponents in one graph per block; "
+                         "prp20m: PRP-3 at the 20M FFT (5 * 2^22)")
     return ap.parse_args()
 
 
@@ -473,11 +474,98 @@ def run_batch64(args, rank, world, local):
     return 0
 
 
+def run_prp20m(args, rank, world, local):
+    """PRP-3 at the 20M FFT (N = 5 * 2^22, W x H = 4096 x 2560, a radix-5 column stage) for E the seeded
+    prime in [330M, 335M]: the same timed steps as the 8M line (modMul(check, data) + one graph-launched
+    block, CUDA events on the plan's stream, L2 flushed between steps), res64 at every 1,000 iterations
+    against the GMP golden table (its first 5,000 iterations) and a Gerbicz check at the end. The
+    proof residues of power 8 lie beyond these iterations (the first at E / 256), so the proof
+    machinery costs nothing here; tests/test_large.py runs the driver with it enabled."""
+    import torch
+    import gpuowl_b200 as owl
+    from gpuowl_b200 import build
+    build.build()
+    torch.cuda.set_device(local)
+    g = load_golden("prp_20m")
+    E = g["E"] if g else 331480451
+    W, H = 4096, 2560
+    N = 2 * W * H
+    B = args.block
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    plan = owl.Plan(E, device=local, W=W, H=H)
+    stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", local))
+    data, check, aux = plan.alloc(), plan.alloc(), plan.alloc()
+    plan.writeIn(data, [3] + [0] * (plan.nwords - 1))
+    plan.writeIn(check, [1] + [0] * (plan.nwords - 1))
+    res, step_ms = [], []
+    prof = {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
+
+    def step():
+        plan.modMul(check, data)
+        return plan.profile_square(data, B)
+
+    for _ in range(args.warmup):
+        step()
+        res.append("%016x" % plan.bufResidue(data))
+    plan.readROE()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pr = step()
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            for k, (ms, n) in pr.items():
+                prof[k][0] += ms
+                prof[k][1] += n
+            res.append("%016x" % plan.bufResidue(data))
+    roe = plan.readROE()
+    plan.squareLoop(aux, check, B, mul3=True)
+    plan.modMul(check, data)
+    gerbicz_ok = plan.isEqual(check, aux)
+    plan.close()
+    n = min(len(res), len(g["res64"])) if g else 0
+    total_ms = sum(step_ms)
+    dom = "pass2" if prof["pass2"][0] >= prof["pass1"][0] else "pass1"
+    avg_ms = prof[dom][0] / max(prof[dom][1], 1)
+    achieved = 16 * N / (avg_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "ms/iter PRP @20M FFT (5*2^22), proof power 8 configured, bit-exact res64",
+        "value": round(total_ms / (args.steps * B), 5), "unit": "ms/iter", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "PRP-3, E=%d (seeded prime in [330M,335M]), FFT 20M (W=4096, H=2560), "
+                               "plain FP64 form" % E,
+                   "E": E, "N": N, "block": B, "step": "modMul(check,data) + %d squarings" % B,
+                   "timed_iterations": args.steps * B, "l2": "flushed (512 MiB write) between timed steps"},
+        "res64_match_golden": (res[:n] == g["res64"][:n]) if g else None, "res64_checked": n,
+        "gerbicz_ok": bool(gerbicz_ok), "max_roe": round(float(roe.max()), 5) if roe.size else None,
+        "kernel_ms": {k: round(v[0] / max(v[1], 1), 5) for k, v in prof.items()},
+        "roofline": {"bound": "hbm", "kernel": "k_pass2" if dom == "pass2" else "k_pass1",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "alg_bytes_per_launch": 16 * N},
+        "gpu_launches": (2 * B + 8) * args.steps,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.workload == "batch64":
         return run_batch64(args, rank, world, local)
+    if args.workload == "prp20m":
+        return run_prp20m(args, rank, world, local)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_ours(args, rank, world, local)
