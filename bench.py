@@ -47,9 +47,9 @@ def parse():
     ap.add_argument("--block", type=int, default=BLOCK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tensor-core) form")
-    ap.add_argument("--workload", default="prp8m", choices=["prp8m", "batch64", "prp20m"],
+    ap.add_argument("--workload", default="prp8m", choices=["prp8m", "batch64", "prp20m", "prp256k"],
                     help="prp8m: the headline line; batch64: 64 uneven exponents in one graph per block; "
-                         "prp20m: PRP-3 at the 20M FFT (5 * 2^22)")
+                         "prp20m / prp256k: PRP-3 at the 20M FFT (5 * 2^22) / the 256K FFT")
     return ap.parse_args()
 
 
@@ -474,21 +474,30 @@ def run_batch64(args, rank, world, local):
     return 0
 
 
-def run_prp20m(args, rank, world, local):
-    """PRP-3 at the 20M FFT (N = 5 * 2^22, W x H = 4096 x 2560, a radix-5 column stage) for E the seeded
-    prime in [330M, 335M]: the same timed steps as the 8M line (modMul(check, data) + one graph-launched
-    block, CUDA events on the plan's stream, L2 flushed between steps), res64 at every 1,000 iterations
-    against the GMP golden table (its first 5,000 iterations) and a Gerbicz check at the end. The
-    proof residues of power 8 lie beyond these iterations (the first at E / 256), so the proof
-    machinery costs nothing here; tests/test_large.py runs the driver with it enabled."""
+# the other PRP configurations: golden table, shape (0 = the library's choice), range of E
+PRP_CONFIGS = {
+    "prp20m": ("prp_20m", 4096, 2560, "20M (5*2^22)", "[330M,335M]",
+               "proof power 8 configured (its first residue point, at E/256, lies beyond the timed "
+               "iterations; tests/test_large.py runs the driver with it)"),
+    "prp256k": ("prp_256k", 0, 0, "256K", "[4.8M,5.0M]", ""),
+}
+
+
+def run_prp_config(args, rank, world, local):
+    """PRP-3 at another configuration (PRP_CONFIGS) for E the seeded prime of its range: the same timed
+    steps as the 8M line (modMul(check, data) + one graph-launched block, CUDA events on the plan's
+    stream, L2 flushed between steps), res64 at every 1,000 iterations against the GMP golden table
+    and a Gerbicz check at the end."""
     import torch
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
     build.build()
     torch.cuda.set_device(local)
-    g = load_golden("prp_20m")
-    E = g["E"] if g else 331480451
-    W, H = 4096, 2560
+    gname, W, H, label, rng_txt, note = PRP_CONFIGS[args.workload]
+    g = load_golden(gname)
+    E = g["E"]
+    if not W:
+        _, W, H = owl.fft_choose(E)
     N = 2 * W * H
     B = args.block
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -537,14 +546,15 @@ def run_prp20m(args, rank, world, local):
     if rank != 0:
         return 0
     line = {
-        "metric": "ms/iter PRP @20M FFT (5*2^22), proof power 8 configured, bit-exact res64",
+        "metric": "ms/iter PRP @%s FFT, bit-exact res64" % label,
         "value": round(total_ms / (args.steps * B), 5), "unit": "ms/iter", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "PRP-3, E=%d (seeded prime in [330M,335M]), FFT 20M (W=4096, H=2560), "
-                               "plain FP64 form" % E,
+        "config": {"workload": "PRP-3, E=%d (seeded prime in %s), FFT %s (W=%d, H=%d), plain FP64 form"
+                               % (E, rng_txt, label, W, H),
                    "E": E, "N": N, "block": B, "step": "modMul(check,data) + %d squarings" % B,
-                   "timed_iterations": args.steps * B, "l2": "flushed (512 MiB write) between timed steps"},
+                   "timed_iterations": args.steps * B, "l2": "flushed (512 MiB write) between timed steps",
+                   "note": note},
         "res64_match_golden": (res[:n] == g["res64"][:n]) if g else None, "res64_checked": n,
         "gerbicz_ok": bool(gerbicz_ok), "max_roe": round(float(roe.max()), 5) if roe.size else None,
         "kernel_ms": {k: round(v[0] / max(v[1], 1), 5) for k, v in prof.items()},
@@ -564,8 +574,8 @@ def main():
     rank, world, local = dist_env()
     if args.workload == "batch64":
         return run_batch64(args, rank, world, local)
-    if args.workload == "prp20m":
-        return run_prp20m(args, rank, world, local)
+    if args.workload in PRP_CONFIGS:
+        return run_prp_config(args, rank, world, local)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_ours(args, rank, world, local)
