@@ -138,6 +138,8 @@ void pass1(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {
     case 128: p1w<128>(p, mode, F, words, flags); break;
     case 256: p1w<256>(p, mode, F, words, flags); break;
     case 512: p1w<512>(p, mode, F, words, flags); break;
+    case 1024: p1w<1024>(p, mode, F, words, flags); break;
+    case 2048: p1w<2048>(p, mode, F, words, flags); break;
     default: throw std::runtime_error("emu W");
   }
   if (mode == P1_OUT) {

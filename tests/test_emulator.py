@@ -48,6 +48,7 @@ def run(exe, *args):
     (110503, 64, 64, 30, 1),      # MUL3 on the last step
     (500009, 128, 128, 24, 0),    # radix-16 first stages, two-level twiddles
     (1300021, 64, 640, 4, 2),     # H = 5 * 128: radix-5 middle stage of the column FFT, LL
+    (4456451, 2048, 64, 3, 0),    # the 8M shape's line pass (2048 points, 16 x 16 x 8) on 64 lines
 ])
 def test_emulated_square_matches_gmp(emu, oracle, E, W, H, n, flags):
     roe, got = run(emu, "square", E, W, H, n, flags, 0)
