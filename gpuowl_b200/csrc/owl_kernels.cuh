@@ -162,11 +162,11 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   OWL_SHARED(uint32_t, s_g);
   OWL_SHARED_ARR(float, s_roe, 32);
 
-  // launched as a programmatic dependent of the column pass: nothing (ticket included) is touched
-  // before that pass has completed
-  griddep_wait();
-  griddep_launch();
-  ts_begin(a, tslot);
+  // Launched as a programmatic dependent of the column pass, a CTA may start before that pass has
+  // completed. It then takes its ticket and reads its tables (nothing that pass writes) before
+  // griddep_wait(), and the state after it. The ticket stays this launch's: the column pass's CTAs
+  // call griddep_launch() only after their own griddep_wait(), so this pass starts no CTA before
+  // the previous line pass, which took and reset the same counter, has completed.
   const int t = threadIdx.x;
   const uint32_t G = a.H / R;
   uint32_t g;
@@ -196,6 +196,9 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
   }
   // word classes of this thread's 32 words (fixed per shape, tabulated on the host)
   const uint2 wmask = __ldg(a.p1masks + (size_t)g * T + t);
+  griddep_wait();
+  griddep_launch();
+  ts_begin(a, tslot);
   // per-line mapping for the inner stages
   const int l = t % R;
   const int tl = t / R;
