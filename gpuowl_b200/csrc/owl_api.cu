@@ -530,7 +530,7 @@ void expand_on_device(owl_plan* p, int32_t* buf, const uint32_t* words) {
      "upload words");
   owl::k_pack_summary<true><<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(p->dwords, nullptr, p->nw, p->E,
                                                                                  p->N, p->packBlk);
-  owl::k_pack_chain<<<1, 32, 0, p->stream>>>(p->packBlk, p->packBlocks, p->packCtl);
+  owl::k_pack_chain<<<1, owl::kPackThreads, 0, p->stream>>>(p->packBlk, p->packBlocks, p->packCtl);
   owl::k_expand_digits<<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(p->dwords, p->nw, p->E, p->N, p->packBlk,
                                                                              p->packCtl, buf);
   ck(cudaGetLastError(), "expand launch");
@@ -578,7 +578,7 @@ void compact_on_device(owl_plan* p, const int32_t* buf, uint32_t* words) {
     ck(cudaMemsetAsync(p->dwords, 0, (size_t)(p->nw + 2) * sizeof(uint32_t), p->stream), "memset words");
     owl::k_pack_summary<false><<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(nullptr, buf, p->nw, p->E, p->N,
                                                                                     p->packBlk);
-    owl::k_pack_chain<<<1, 32, 0, p->stream>>>(p->packBlk, p->packBlocks, p->packCtl);
+    owl::k_pack_chain<<<1, owl::kPackThreads, 0, p->stream>>>(p->packBlk, p->packBlocks, p->packCtl);
     owl::k_compact_words<<<p->packBlocks, owl::kPackThreads, 0, p->stream>>>(buf, p->nw, p->E, p->N, p->packBlk,
                                                                                p->packCtl, p->dwords);
     owl::k_compact_finish<<<1, 32, 0, p->stream>>>(p->packCtl, p->nw, p->dwords);

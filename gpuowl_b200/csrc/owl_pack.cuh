@@ -91,17 +91,38 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_summary(const uint32_t* _
   }
 }
 
-// K2: block carries in, in order; blk[b] becomes the carry into block b (0/1)
-static __global__ void k_pack_chain(uint32_t* __restrict__ blk, uint32_t nblocks, PackCtl* ctl) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) { return; }
-  uint32_t c = 0;
-  for (uint32_t b = 0; b < nblocks; ++b) {
-    const uint32_t s = blk[b];
-    blk[b] = c;
-    c = (s == ST_PROP) ? c : s;
+// K2: block carries in, in order; blk[b] becomes the carry into block b (0/1). One CTA of
+// kPackThreads threads: each thread composes the statuses of its run of consecutive blocks, the runs'
+// statuses are scanned in shared memory (Hillis-Steele with pk_compose, which is associative), and
+// each thread then walks its run with the carry into it. A single thread walking all the blocks
+// would make one dependent global load per 1,024 digits (8,192 in a row at 8M).
+static __global__ void __launch_bounds__(kPackThreads) k_pack_chain(uint32_t* __restrict__ blk, uint32_t nblocks,
+                                                                    PackCtl* ctl) {
+  OWL_SHARED_ARR(uint32_t, s_run, kPackThreads);
+  const uint32_t t = threadIdx.x;
+  const uint32_t per = (nblocks + kPackThreads - 1) / kPackThreads;
+  const uint32_t lo = (t * per < nblocks) ? t * per : nblocks;
+  const uint32_t hi = (lo + per < nblocks) ? lo + per : nblocks;
+  uint32_t agg = ST_PROP;  // an empty run propagates
+  for (uint32_t b = lo; b < hi; ++b) { agg = pk_compose(agg, blk[b]); }
+  s_run[t] = agg;
+  __syncthreads();
+  for (uint32_t off = 1; off < kPackThreads; off <<= 1) {
+    const uint32_t v = (t >= off) ? pk_compose(s_run[t - off], s_run[t]) : s_run[t];
+    __syncthreads();
+    s_run[t] = v;
+    __syncthreads();
   }
-  ctl->carryOut = c;
-  ctl->error = 0;
+  // carry into this run: the composed status of all runs below; none below, or all propagating: 0
+  uint32_t c = (t == 0) ? (uint32_t)ST_KILL : s_run[t - 1];
+  if (c == ST_PROP) { c = ST_KILL; }
+  for (uint32_t b = lo; b < hi; ++b) {
+    const uint32_t st = blk[b];
+    blk[b] = c;
+    c = (st == ST_PROP) ? c : st;
+  }
+  if (lo < hi && hi == nblocks) { ctl->carryOut = c; }
+  if (t == 0) { ctl->error = 0; }
 }
 
 // carry into this thread's first digit: the nearest non-propagating thread below, else the block's

@@ -6,6 +6,7 @@
 //   owl_emu square E W H n flags seed   (seed 0: start from 3, or 4 with LL)
 //   owl_emu modmul E W H mul3 seedA seedB
 //   owl_emu pack E N pattern            (device expand / compact vs owl_words.hpp; prints "pack ok")
+//   owl_emu chain nblocks seed          (the block-carry chain vs its serial definition; "chain ok")
 // With OWL_EMU_SPLIT=1 in the environment and H = 2048 the column pass runs the
 // split-precision kernel (k_pass2_tc) on the emulated tensor cores.
 // Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
@@ -254,7 +255,7 @@ int pack_test(uint32_t E, uint32_t N, uint64_t pattern) {
   int32_t* pd = dev.data();
   PackCtl* pc = &ctl;
   emu_launch(nb, kPackThreads, 0, [=] { k_pack_summary<true>(pw, nullptr, nw, E, N, pb); });
-  emu_launch(1, 32, 0, [=] { k_pack_chain(pb, nb, pc); });
+  emu_launch(1, kPackThreads, 0, [=] { k_pack_chain(pb, nb, pc); });
   emu_launch(nb, kPackThreads, 0, [=] { k_expand_digits(pw, nw, E, N, pb, pc, pd); });
   if (dev != host) {
     std::printf("error expand differs\n");
@@ -265,7 +266,7 @@ int pack_test(uint32_t E, uint32_t N, uint64_t pattern) {
   const int32_t* ph = host.data();
   uint32_t* po = dwords.data();
   emu_launch(nb, kPackThreads, 0, [=] { k_pack_summary<false>(nullptr, ph, nw, E, N, pb); });
-  emu_launch(1, 32, 0, [=] { k_pack_chain(pb, nb, pc); });
+  emu_launch(1, kPackThreads, 0, [=] { k_pack_chain(pb, nb, pc); });
   emu_launch(nb, kPackThreads, 0, [=] { k_compact_words(ph, nw, E, N, pb, pc, po); });
   emu_launch(1, 32, 0, [=] { k_compact_finish(pc, nw, po); });
   if (ctl.error || !std::equal(want.begin(), want.end(), dwords.begin())) {
@@ -276,10 +277,41 @@ int pack_test(uint32_t E, uint32_t N, uint64_t pattern) {
   return 0;
 }
 
+// the block-carry chain alone on nb random statuses (runs of propagating blocks included), against
+// the serial definition: carry into block b = the last non-propagating status below b, else 0
+int chain_test(uint32_t nb, uint64_t seed) {
+  std::vector<uint32_t> st(nb), blk(nb), want(nb);
+  uint64_t sd = seed;
+  for (uint32_t b = 0; b < nb; ++b) {
+    const uint64_t r = splitmix(sd) % 8;
+    st[b] = r < 5 ? (uint32_t)ST_PROP : (r < 7 ? (uint32_t)ST_KILL : (uint32_t)ST_GEN);
+  }
+  uint32_t c = 0;
+  for (uint32_t b = 0; b < nb; ++b) {
+    want[b] = c;
+    c = (st[b] == ST_PROP) ? c : st[b];
+  }
+  blk = st;
+  PackCtl ctl{};
+  ctl.carryOut = 7;
+  uint32_t* pb = blk.data();
+  PackCtl* pc = &ctl;
+  emu_launch(1, kPackThreads, 0, [=] { k_pack_chain(pb, nb, pc); });
+  if (blk != want || ctl.carryOut != c) {
+    std::printf("error chain differs\n");
+    return 7;
+  }
+  std::printf("chain ok\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) { return 2; }
   std::string mode = argv[1];
   try {
+    if (mode == "chain" && argc == 4) {
+      return chain_test(std::strtoul(argv[2], nullptr, 10), std::strtoull(argv[3], nullptr, 10));
+    }
     if (mode == "pack" && argc == 5) {
       return pack_test(std::strtoul(argv[2], nullptr, 10), std::strtoul(argv[3], nullptr, 10),
                        std::strtoull(argv[4], nullptr, 10));

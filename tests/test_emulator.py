@@ -113,6 +113,15 @@ def test_emulated_split_precision_column_pass(emu, oracle, mode):
     assert 0 < float(lines[0].split()[1]) < 0.1
 
 
+@pytest.mark.parametrize("nb,seed", [(1, 1), (17, 2), (256, 3), (257, 4), (8192, 5), (20480, 6)])
+def test_emulated_pack_chain(emu, nb, seed):
+    """The block-carry chain of the word conversion (one CTA: per-thread runs of blocks, a scan of
+    the runs, then each run walked with its carry in) against its serial definition."""
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")
+    r = subprocess.run([emu, "chain", str(nb), str(seed)], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0 and r.stdout.strip() == "chain ok", (r.stdout[-500:], r.stderr[-2000:])
+
+
 @pytest.mark.parametrize("E,N,pattern", [(216091, 16384, p) for p in range(6)] + [(327691, 20480, 2)])
 def test_emulated_device_expand_compact(emu, E, N, pattern):
     """owl_pack.cuh kernels against owl_words.hpp (3, 2^E-1, an all-propagating carry, 0, 2^E-2, random)."""
