@@ -14,7 +14,8 @@ with the GMP golden table and a full Gerbicz check (B extra squarings) is run.
 
 --impl reference times the reference's algorithm on the host cores: the reference's
 OpenCL kernels cannot run here, so its CPU restatement (oracle/ibdwt.c, all host
-threads) stands in, one 8M squaring per step. Multi-GPU runs are replicas (one
+threads) stands in, timed over a fixed sample of CPU_SAMPLE 8M squarings; the other arm
+takes the same sample for its cpu_baseline before it touches the GPU. Multi-GPU runs are replicas (one
 exponent per GPU, no collective on the data path): value = max-over-ranks time /
 all iterations.
 """
@@ -36,6 +37,9 @@ W_8M, H_8M = 2048, 2048
 N_8M = 2 * W_8M * H_8M
 NW_8M = (E_8M - 1) // 32 + 1
 BLOCK = 1000
+# squarings in the CPU sample (after one untimed squaring), the same in both arms: about 2 s of
+# CPU work at 8M on 16 host threads
+CPU_SAMPLE = 25
 
 
 def parse():
@@ -199,30 +203,43 @@ def replica_summary(dist, total_ms, e2e_step_ms, steps, block, world, device="cp
     return total_ms, e2e_step_ms, total_ms / (world * steps * block)
 
 
+def cpu_sample_line():
+    """The CPU baseline: CPU_SAMPLE squarings of the 8M workload with oracle/ibdwt.c on every host
+    thread. Both arms take it the same way, in a process that has not touched the GPU yet."""
+    threads = os.cpu_count() or 1
+    ms, _ = cpu_port_ms_per_iter(E_8M, N_8M, CPU_SAMPLE, threads)
+    return {"value": round(ms, 3), "unit": "ms/iter", "cores": threads, "kind": "port",
+            "sample": "%d squarings (after 1 untimed) at E=%d, N=8M with oracle/ibdwt.c (OpenMP, all host "
+                      "threads), taken before any GPU work; the reference's OpenCL kernels have no CPU "
+                      "runtime here" % (CPU_SAMPLE, E_8M)}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
-    iters = args.warmup + args.steps
-    ms, _ = cpu_port_ms_per_iter(E_8M, N_8M, iters, threads)
+    cpu = cpu_sample_line()
+    ms = cpu["value"]
     line = {
         "impl": "reference",
         "metric": "ms/iter PRP @8M FFT: split-precision TC vs plain FP64, bit-exact res64",
-        "value": round(ms, 3), "unit": "ms/iter", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "value": ms, "unit": "ms/iter", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "PRP-3 squaring, E=136181029 (seeded prime in [136M,139M]), FFT 8M",
-                   "E": E_8M, "N": N_8M, "step": "one 8M IBDWT squaring on the host cores"},
-        "cpu_baseline": {"value": round(ms, 3), "unit": "ms/iter", "cores": threads, "kind": "port",
-                         "sample": "%d squarings at E=%d, N=8M (oracle/ibdwt.c, OpenMP); the reference's "
-                                   "OpenCL kernels have no CPU runtime here" % (iters, E_8M)},
-        "e2e": {"value": round(ms, 3), "unit": "ms/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                   "E": E_8M, "N": N_8M, "step": "one 8M IBDWT squaring on the host cores",
+                   "sample": "%d squarings regardless of --steps/--warmup" % CPU_SAMPLE},
+        "cpu_baseline": cpu,
+        "e2e": {"value": ms, "unit": "ms/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_ours(args, rank, world, local):
+    # the CPU baseline first, in a process that has not touched the GPU (rank 0 of a 1-GPU run)
+    cpu = None
+    if not args.no_cpu_baseline and world == 1 and rank == 0:
+        cpu = cpu_sample_line()
     import numpy as np
     import torch
     import gpuowl_b200 as owl
@@ -363,14 +380,6 @@ def run_ours(args, rank, world, local):
         if dist is not None:
             dist.destroy_process_group()
         return 0
-
-    cpu = None
-    if not args.no_cpu_baseline and world == 1:
-        iters = 12
-        ms, _ = cpu_port_ms_per_iter(E_8M, N_8M, iters, os.cpu_count() or 1)
-        cpu = {"value": round(ms, 2), "unit": "ms/iter", "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": "%d squarings at E=%d, N=8M with oracle/ibdwt.c (OpenMP, all host threads)"
-                         % (iters, E_8M)}
 
     # per timed step: modMul = pass1 IN, pass2 FWD, pass1 IN, pass2 MUL, pass1 OUT, carry fixup (6);
     # the block = pass1 IN, B x pass2, B-1 x pass1 FUSED, pass1 OUT, carry fixup (2B + 2)

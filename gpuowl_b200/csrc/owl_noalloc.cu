@@ -1,29 +1,35 @@
 // owl_noalloc.cu -- owl_square_noalloc: n squarings of a caller's word buffer
 // with no allocation at all.
 //
-// Some callers cannot allocate device memory: code running while a CUDA graph
-// is being captured (where cudaMalloc is not allowed), hosts that hand all
-// device memory to their own pool allocator, and real-time loops that must not
-// enter the allocator. For them this entry point keeps every piece of scratch
-// the squaring needs -- the FFT state, the carry rows and flags, the control
-// word, the twiddle and weight tables -- in one file-scope device array of a
-// fixed size, so the library never calls cudaMalloc, cudaFree or any other
-// allocating routine on this path (the tables are computed on the device).
+// Some callers of this library cannot allocate device memory: a host that has
+// handed all device memory to its own pool allocator (a cudaMalloc would fail,
+// or take memory the pool counts on), a real-time loop that must not enter the
+// allocator (cudaMalloc and cudaFree can block on the device and take an
+// unbounded time), and plug-ins whose host forbids them to allocate. For them
+// this entry point keeps every piece of scratch the squaring needs -- the FFT
+// state, the carry rows and flags, the control word, the twiddle and weight
+// tables -- in one file-scope device array of a fixed size, so the library
+// never calls cudaMalloc, cudaFree or any other allocating routine on this path
+// (the tables are computed on the device).
 //
 // Limits and rules:
-//   - N = 2 W H <= kNoAllocMaxWords (W <= 128, H <= 256: exponents up to about
-//     1.2 million at 19 bits per word); larger shapes return OWL_ERR_ARG;
+//   - N = 2 W H <= kNoAllocMaxWords (W <= 128, H <= 256) and at most 19 bits
+//     per word (exponents up to about 1.24 million); anything else returns
+//     OWL_ERR_ARG;
 //   - the array (kNoAllocScratchBytes) lives on every GPU that loads libowl
 //     until the process exits;
 //   - every call shares that one array and it keeps the last call's contents;
 //     the call clears what must start at zero, but calls that overlap on the
 //     GPU (other streams, other host threads) race on it and corrupt each other;
 //   - the first call on a device looks up the array's device address (with
-//     that device current) and caches it; make that first call outside any
-//     stream capture.
+//     that device current) and caches it; make that first call before any
+//     stream capture;
+//   - the call waits for its work on `stream` and reads back the device-side
+//     status and the round-off maximum.
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 #include <cstdint>
 #include <mutex>
 
@@ -43,6 +49,9 @@ constexpr uint32_t kNoAllocMaxH = 256;
 constexpr size_t kNoAllocScratchBytes = 1u << 20;
 constexpr int kR = 2;
 constexpr uint32_t kRoeSlots = 16;
+constexpr double kNoAllocMaxBpw = 19.0;
+// a round-off above this means the FFT was too short for the exponent; the call fails
+constexpr float kNoAllocMaxRoe = 0.4f;
 
 // The scratch array. Its name is a host-side stand-in in host code: kernels
 // get the address looked up with cudaGetSymbolAddress, never &g_noalloc_scratch.
@@ -204,7 +213,7 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
     // smallest shape of this path with at most 19 bits per word
     const uint32_t shapes[4][2] = {{64, 64}, {64, 128}, {128, 128}, {128, 256}};
     for (const auto& sh : shapes) {
-      if ((double)E / (2.0 * sh[0] * sh[1]) <= 19.0) {
+      if ((double)E / (2.0 * sh[0] * sh[1]) <= kNoAllocMaxBpw) {
         W = sh[0];
         H = sh[1];
         break;
@@ -218,8 +227,10 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
   }
   const uint32_t N = 2 * W * H;
   if (N > kNoAllocMaxWords) { return fail(OWL_ERR_ARG, "no-alloc path: FFT larger than its fixed scratch (N <= 65536)"); }
-  if (E < 1000 || E % 2 == 0 || E / N < 8 || (double)E / N > 21.0) {
-    return fail(OWL_ERR_ARG, "no-alloc path: exponent out of range for this FFT");
+  // the same 19-bit limit as the automatic choice: these small transforms are not shown to keep the
+  // round-off safe above it
+  if (E < 1000 || E % 2 == 0 || E / N < 8 || (double)E / N > kNoAllocMaxBpw) {
+    return fail(OWL_ERR_ARG, "no-alloc path: exponent out of range for this FFT (8 to 19 bits per word)");
   }
   if (device < 0 || device >= kMaxDevices) { return fail(OWL_ERR_NODEV, "device ordinal out of range"); }
   int prev = -1;
@@ -229,6 +240,12 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
     int prev, dev;
     ~Restore() { if (prev >= 0 && prev != dev) { cudaSetDevice(prev); } }
   } restore{prev, device};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread) {
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) { return fail(OWL_ERR_ARG, "no-alloc path: invalid stream"); }
+    if (sdev != device) { return fail(OWL_ERR_ARG, "no-alloc path: stream belongs to another device"); }
+  }
 
   unsigned char* base = nullptr;
   {
@@ -278,7 +295,6 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
   a.loShift = loShift;
   a.timeoutNs = 2000000000ull;
   owl::C* F = reinterpret_cast<owl::C*>(base + L.F);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   const int twWn = owl::tw_offsets((int)W, 16 / kR).total, twHn = owl::tw_offsets((int)H, 8).total;
   k_noalloc_tables<<<64, 256, 0, s>>>(a, (uint32_t)twWn, (uint32_t)twHn);
@@ -293,12 +309,25 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
     owl::k_carry_fixup<<<1, 32, 0, s>>>(a, words);
   }
   if (cudaGetLastError() != cudaSuccess) { return fail(OWL_ERR_CUDA, "launch failed"); }
-  // the device-side wait status is read back so the caller learns of a timeout
-  uint32_t err = 0;
-  if (cudaMemcpyAsync(&err, &a.ctl->error, sizeof(err), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+  // the device-side status word and the round-off slots are read back in one copy (the control
+  // word comes first in the scratch, the round-off slots right after it)
+  static_assert(sizeof(owl::Ctl) <= 256, "control word layout");
+  unsigned char back[256 + kRoeSlots * sizeof(float)];
+  if (L.roe != L.ctl + 256 ||
+      cudaMemcpyAsync(back, base + L.ctl, sizeof(back), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess) {
     return fail(OWL_ERR_CUDA, "synchronize failed");
   }
-  if (err) { return fail(OWL_ERR_TIMEOUT, "device-side carry wait timed out"); }
+  owl::Ctl ctl;
+  float roe[kRoeSlots];
+  std::memcpy(&ctl, back, sizeof(ctl));
+  std::memcpy(roe, back + 256, sizeof(roe));
+  if (ctl.error & owl::DEVERR_WAIT) { return fail(OWL_ERR_TIMEOUT, "device-side carry wait timed out"); }
+  if (ctl.error & owl::DEVERR_PENDING) {
+    return fail(OWL_ERR_CUDA, "no-alloc path: the leftover-carry queue of the last pass overflowed");
+  }
+  if (n > 0 && !(roe[kRoeSlots - 1] <= kNoAllocMaxRoe)) {
+    return fail(OWL_ERR_ARG, "no-alloc path: round-off above 0.4, the FFT is too short for this exponent");
+  }
   return OWL_OK;
 }

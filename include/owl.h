@@ -153,18 +153,18 @@ int owl_batch_destroy(owl_batch* batch);
 
 /* No counterpart in the reference (its host allocates every device buffer up front).
    n squarings (flags as for owl_square) of `words`, a device buffer of N = 2*W*H balanced int32
-   digits on `device`, in place, queued on `stream` (a cudaStream_t; NULL is the legacy default
-   stream) -- without allocating anything. It is meant for callers that cannot call cudaMalloc:
-   code running inside a CUDA graph capture, programs whose device memory all belongs to their
-   own pool allocator, and real-time loops that must stay out of the allocator. All scratch (FFT
-   state, carry rows, tables) lives in one fixed 1 MiB device array inside libowl, present on every
-   GPU that loads the library until the process exits, so only small FFTs fit: W in {64, 128},
-   H in {64, 128, 256}, N <= 65536 (W = H = 0 picks the smallest that holds E at <= 19 bits per
-   word); anything larger returns OWL_ERR_ARG. Every call shares that array and it keeps the last
-   call's contents: calls that overlap on the GPU race and corrupt each other. The first call on a
-   device looks up the array's address with that device current; make it before any stream
-   capture. The call waits for its work and reports a device-side wait timeout as OWL_ERR_TIMEOUT;
-   the error text is in owl_last_error(). */
+   digits on `device`, in place, queued on `stream` (a cudaStream_t of that device; NULL is the
+   legacy default stream) -- without allocating anything. It is meant for callers that cannot call
+   cudaMalloc: hosts whose device memory all belongs to their own pool allocator, real-time loops
+   that must not block in the allocator, and plug-ins whose host forbids allocation. All scratch
+   (FFT state, carry rows, tables) lives in one fixed 1 MiB device array inside libowl, present on
+   every GPU that loads the library until the process exits, so only small FFTs fit: W in {64, 128},
+   H in {64, 128, 256}, N <= 65536, at most 19 bits per word (W = H = 0 picks the smallest shape
+   that holds E); anything larger returns OWL_ERR_ARG. Every call shares that array and it keeps
+   the last call's contents: calls that overlap on the GPU race and corrupt each other. The first
+   call on a device looks up the array's address with that device current; make it before any
+   stream capture. The call waits for its work; a device-side wait timeout returns
+   OWL_ERR_TIMEOUT, a round-off above 0.4 OWL_ERR_ARG; the error text is in owl_last_error(). */
 int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H, int32_t* words, uint32_t n,
                        uint32_t flags, void* stream);
 
