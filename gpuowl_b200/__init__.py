@@ -53,7 +53,9 @@ class RunResult(ctypes.Structure):
     """owl_run_result (include/owl_host.h)."""
     _fields_ = [("is_prime", ctypes.c_int), ("finished", ctypes.c_int), ("k", ctypes.c_uint32),
                 ("res64", ctypes.c_uint64), ("n_errors", ctypes.c_uint32), ("res2048", ctypes.c_char * 513),
-                ("proof_power", ctypes.c_uint32), ("proof_file", ctypes.c_char * 1024)]
+                ("proof_power", ctypes.c_uint32), ("proof_file", ctypes.c_char * 1024),
+                ("roe_n", ctypes.c_uint32), ("roe_max", ctypes.c_float), ("roe_z", ctypes.c_float),
+                ("roe_z_avg", ctypes.c_float), ("n_danger_roe", ctypes.c_uint32)]
 
 
 _SIGS = {
@@ -338,6 +340,8 @@ def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, 
     return {"is_prime": bool(r.is_prime), "finished": bool(r.finished), "k": r.k, "res64": r.res64,
             "n_errors": r.n_errors, "res2048": r.res2048.decode(),
             "proof_power": r.proof_power, "proof_file": r.proof_file.decode() or None,
+            "roe_n": r.roe_n, "roe_max": r.roe_max, "roe_z": r.roe_z, "roe_z_avg": r.roe_z_avg,
+            "n_danger_roe": r.n_danger_roe,
             "checkpoints": [(ks[i], rs[i]) for i in range(n.value)]}
 
 

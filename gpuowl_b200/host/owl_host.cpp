@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <array>
 #include <cinttypes>
+#include <cmath>
 #include <memory>
 #include <cstdarg>
 #include <cstdio>
@@ -360,6 +361,14 @@ class HostGpu {
     return r;
   }
   void copy(int32_t* dst, const int32_t* src) { ck(owl_buf_copy(plan_, dst, src)); }
+  // per-squaring round-off maxima recorded since the last call (Gpu::readROE, src/Gpu.cpp:624-637)
+  std::vector<float> readRoe() {
+    std::vector<float> v(1u << 16);
+    uint32_t n = 0;
+    ck(owl_read_roe(plan_, v.data(), (uint32_t)v.size(), &n));
+    v.resize(n);
+    return v;
+  }
 
   // src/Gpu.cpp:738-765: data = 3 * check^(2^B - 1), rebuilt from the saved check
   void writeState(const Words& checkWords, uint32_t B) {
@@ -717,6 +726,64 @@ std::string hex64words(const Words& w) {
   return s;
 }
 
+// Round-off statistics of a sample of per-squaring maxima (src/Gpu.cpp:311-327 roeStat and the
+// RoeInfo Gumbel fit of src/Gpu.h:62-81): beta = sd * sqrt(6) / pi, miu = mean - gamma * beta,
+// Z(x) = (x - miu) / beta.
+struct RoeInfo {
+  uint32_t N = 0;
+  double max = 0, mean = 0, sd = 0, beta = 0, miu = 0;
+  explicit RoeInfo(const std::vector<float>& v) {
+    double sum = 0, sum2 = 0;
+    for (float f : v) {
+      const double x = f;
+      max = std::max(max, x);
+      sum += x;
+      sum2 += x * x;
+    }
+    N = (uint32_t)v.size();
+    if (!N) { return; }
+    sd = std::sqrt(std::max(0.0, N * sum2 - sum * sum)) / N;
+    mean = sum / N;
+    beta = sd * 0.779696801233676;       // sqrt(6) / pi
+    miu = mean - beta * 0.577215664901533;  // Euler-Mascheroni
+  }
+  double z(double x = 0.5) const { return N && beta > 0 ? (x - miu) / beta : 0.0; }
+};
+
+// Which squaring blocks feed the statistics: the reference measures the round-off on a few
+// iterations only (wantROE, src/Gpu.cpp:1459-1464, 1026): 2,000 iterations once the first 30 of a
+// run are past, then 400 after every log step. Blocks are sampled whole here.
+struct RoeSampler {
+  uint32_t skipTo = 0;
+  uint32_t want = 0;
+  std::vector<float> sample;
+  double zSum = 0, zN = 0;
+  void start(uint32_t startK) {
+    skipTo = startK + 30;
+    want = 2000;
+  }
+  bool takes(uint32_t k) const { return want > 0 && k >= skipTo; }
+  void add(uint32_t iters, std::vector<float> v) {
+    want = iters >= want ? 0 : want - iters;
+    sample.insert(sample.end(), v.begin(), v.end());
+  }
+  // the statistics of the sample since the last log step; records them in the run result
+  RoeInfo logStep(owl_run_result& res) {
+    RoeInfo info(sample);
+    sample.clear();
+    want = 400;
+    if (info.N) {
+      res.roe_n += info.N;
+      res.roe_max = std::max(res.roe_max, (float)info.max);
+      res.roe_z = (float)info.z();
+      zSum += info.z() * info.N;
+      zN += info.N;
+      res.roe_z_avg = (float)(zSum / zN);
+    }
+    return info;
+  }
+};
+
 struct Log {
   const owl_run_opts& o;
   void checkpoint(uint32_t k, uint64_t res) {
@@ -781,6 +848,8 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
       if (power) { proofSet = std::make_unique<ProofSet>(o.save_dir, E, power); }
     }
     uint32_t persistK = proofSet ? proofSet->next(k) : UINT32_MAX;
+    RoeSampler roe;
+    roe.start(startK);
     bool skipNextCheckUpdate = false;
     bool reload = false;
     Words finalWords;
@@ -794,7 +863,10 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
       uint32_t next = roundUp(k + 1, B);
       if (k < kEnd && kEnd < next) { next = kEnd; }
       if (persistK > k && persistK < next) { next = persistK; }
+      const bool sample = roe.takes(k);
+      if (sample) { gpu.readRoe(); }  // drops what the modMul recorded
       gpu.squareLoop(gpu.data, gpu.data, next - k);
+      if (sample) { roe.add(next - k, gpu.readRoe()); }
       k = next;
       if (k == persistK) {
         proofSet->save(k, gpu.readOut(gpu.data));
@@ -821,10 +893,17 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
       if (!doCheck && !doLog) { continue; }
       const uint64_t r = gpu.residue(gpu.data);
       log.checkpoint(k, r);
+      // src/Gpu.cpp:1011-1025 doBigLog: Z of the sampled round-off, and the danger warning
+      const RoeInfo ri = roe.logStep(res);
+      const std::string zs = ri.N ? fmt(" Z=%.0f (avg %.1f)", ri.z(), (double)res.roe_z_avg) : std::string();
+      if (ri.N > 2 && ri.z() < 20) {
+        ++res.n_danger_roe;
+        log.line(fmt("Danger ROE! Z=%.1f is too small, increase precision or FFT size!", ri.z()));
+      }
       Words rawCheck = gpu.readOut(gpu.check);
       if (!doCheck) {
         if (saver.enabled()) { saver.savePrpUnverified({E, k, B, r, rawCheck, nErrors, 0}); }
-        log.line(fmt("   %9u %016" PRIx64, k, r));
+        log.line(fmt("   %9u %016" PRIx64 "%s", k, r, zs.c_str()));
         continue;
       }
       const bool ok = gpu.doCheck(B);
@@ -832,7 +911,7 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
         nSeqErrors = 0;
         skipNextCheckUpdate = true;
         if (k < kEnd && saver.enabled()) { saver.savePrp({E, k, B, r, rawCheck, nErrors, 0}); }
-        log.line(fmt("OK %9u %016" PRIx64, k, r));
+        log.line(fmt("OK %9u %016" PRIx64 "%s", k, r, zs.c_str()));
         if (k >= kEndEnd) {
           if (proofSet) {
             const fs::path pf = save_proof(gpu, *proofSet, o.save_dir);
@@ -847,7 +926,7 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
         }
       } else {
         ++nErrors;
-        log.line(fmt("EE %9u %016" PRIx64 " (check failed, %u errors)", k, r, nErrors));
+        log.line(fmt("EE %9u %016" PRIx64 "%s (check failed, %u errors)", k, r, zs.c_str(), nErrors));
         if (++nSeqErrors > 2) { fail(OWL_ERR_READ, "too many errors"); }
         if (r == lastFailedRes64) { fail(OWL_ERR_READ, "consistent error"); }
         lastFailedRes64 = r;
@@ -886,11 +965,21 @@ void ll(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
     uint32_t k = st.k;
     const uint32_t startK = k, kEnd = E - 2;
     bool reload = false;
+    // round-off statistics per log step (the reference computes none in its LL loop, src/Gpu.cpp:1588;
+    // the same Z and danger warning as the PRP loop's are logged here)
+    RoeSampler roe;
     while (true) {
       uint32_t next = roundUp(k + 1, logStep);
       if (next > kEnd) { next = kEnd; }
       if (o.stop_after && next - startK > o.stop_after) { next = std::max(k + 1, startK + o.stop_after); }
       gpu.squareLoop(gpu.data, gpu.data, next - k, OWL_SQ_LL);
+      {
+        // slot i holds squaring i of this call; the first 30 of the run are left out, as in the PRP loop
+        std::vector<float> rv = gpu.readRoe();
+        const size_t skip = k - startK < 30 ? std::min<size_t>(30 - (k - startK), rv.size()) : 0;
+        rv.erase(rv.begin(), rv.begin() + skip);
+        roe.add(next - k, std::move(rv));
+      }
       k = next;
       const bool doStop = (k >= kEnd) || (o.stop_after && k - startK >= o.stop_after);
       Words w = gpu.readOut(gpu.data);
@@ -909,7 +998,13 @@ void ll(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
       }
       if (!isZero && saver.enabled()) { saver.saveLL({E, k, w, 0}); }
       log.checkpoint(k, r);
-      log.line(fmt("%9u %016" PRIx64, k, r));
+      const RoeInfo ri = roe.logStep(res);
+      if (ri.N > 2 && ri.z() < 20) {
+        ++res.n_danger_roe;
+        log.line(fmt("Danger ROE! Z=%.1f is too small, increase precision or FFT size!", ri.z()));
+      }
+      log.line(fmt("%9u %016" PRIx64 "%s", k, r,
+                   ri.N ? fmt(" Z=%.0f (avg %.1f)", ri.z(), (double)res.roe_z_avg).c_str() : ""));
       if (k >= kEnd) {
         res.is_prime = isZero;
         res.res64 = r;

@@ -2,6 +2,7 @@
 each FFT with Gpu::timePRP and writes tune.txt).
 
     python -m gpuowl_b200.tune [--min-lg 13] [--max-lg 23] [--iters 200] [--out tune.txt]
+    python -m gpuowl_b200.tune --bpw-scan tune.json [--criterion z|roe] --out bpw.txt
 
 For every FFT size N = 2^lg, and N = 5 * 2^(lg-3) with --five, it times each W x H split the library
 supports (W a power of two in [64, 4096]; H a power of two in [64, 4096] with H/W in {1/2, 1, 2, 4},
@@ -142,6 +143,144 @@ def roe_at(N, W, H, bpw, iters, device=0):
         return float(p.readROE().max())
 
 
+def is_prime(n):
+    """Deterministic Miller-Rabin for n < 3.3e24 (the bases 2..41)."""
+    if n < 2:
+        return False
+    small = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41)
+    for p in small:
+        if n % p == 0:
+            return n == p
+    d, s = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        s += 1
+    for a in small:
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(s - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def prev_prime(n):
+    """The largest odd prime below n (Primes::prevPrime, src/Primes.cpp:37-43)."""
+    n = int(n) - 1
+    n -= (n % 2 == 0)
+    while not is_prime(n):
+        n -= 2
+    return n
+
+
+def next_prime(n):
+    """The smallest odd prime above n (Primes::nextPrime, src/Primes.cpp:45-50)."""
+    n = int(n) + 1
+    n += (n % 2 == 0)
+    while not is_prime(n):
+        n += 2
+    return n
+
+
+def roe_z(values, x=0.5):
+    """Z of a sample of per-squaring round-off maxima: the reference's Gumbel fit (RoeInfo,
+    src/Gpu.h:62-81; roeStat, src/Gpu.cpp:311-327): beta = sd sqrt(6)/pi, miu = mean - gamma beta,
+    Z = (x - miu) / beta."""
+    import math
+    n = len(values)
+    if n == 0:
+        return 0.0
+    s = sum(float(v) for v in values)
+    s2 = sum(float(v) * float(v) for v in values)
+    sd = math.sqrt(max(0.0, n * s2 - s * s)) / n
+    beta = sd * 0.779696801233676
+    miu = s / n - beta * 0.577215664901533
+    return (x - miu) / beta if beta > 0 else 0.0
+
+
+def z_for_bpw(N, W, H, bpw, count=1, device=0, block=200, iters=2000, warmup=50):
+    """The reference's Tune::zForBpw (src/tune.cpp:174-186) with its measureROE loop (Gpu.cpp:1276-1320:
+    50 warm-up squarings, then 2,000 in blocks of 200): Z of the per-squaring round-off at
+    E = prevPrime(N bpw) (count 1) or the `count` primes after N bpw, averaged."""
+    import numpy as np
+    import gpuowl_b200 as owl
+    E = prev_prime(N * bpw) if count == 1 else next_prime(N * bpw)
+    total = 0.0
+    for _ in range(count):
+        with owl.Plan(E, device=device, W=W, H=H) as p:
+            b = p.alloc()
+            p.writeIn(b, [3] + [0] * (p.nwords - 1))
+            p.squareLoop(b, b, warmup)
+            p.readROE()
+            sample = []
+            for _ in range(iters // block):
+                p.squareLoop(b, b, block)
+                sample.extend(float(v) for v in p.readROE())
+        total += roe_z(sample)
+        E = next_prime(E + 1)
+    return total / count
+
+
+def max_bpw_z(N, W, H, guess, device=0, target=28.0, sample_size=5, verbose=True):
+    """Tune::maxBpw (src/tune.cpp:106-172): bits per word at which the round-off Z is `target` (28).
+    A secant search finds a bpw with Z in [31, 37] and one with Z in [20, 25], each re-measured on
+    `sample_size` exponents; the result interpolates between the two. `guess` is where the search
+    starts (the reference starts 9 steps below its table's value)."""
+    import math
+    step = 0.015 + (math.log2(N) - math.log2(4.0 * 1024 * 1024)) / \
+        (math.log2(7.5 * 1024 * 1024) - math.log2(4.0 * 1024 * 1024)) * (0.012 - 0.015)
+    step = min(max(step, 0.005), 0.05)
+
+    def search(bpw, lo, hi, aim):
+        nonlocal step
+        z = z_for_bpw(N, W, H, bpw, 1, device)
+        if verbose:
+            print("N=%-9d %-14s bpw %.3f  Z %.2f" % (N, spec(W, H), bpw, z), flush=True)
+        for _ in range(40):
+            if lo <= z <= hi:
+                break
+            prev_bpw, prev_z = bpw, z
+            bpw = bpw + (z - aim) * step
+            z = z_for_bpw(N, W, H, bpw, 1, device)
+            if verbose:
+                print("N=%-9d %-14s bpw %.3f  Z %.2f" % (N, spec(W, H), bpw, z), flush=True)
+            if z != prev_z:
+                step = min(max(-(bpw - prev_bpw) / (z - prev_z), 0.005), 0.025)
+        z = (z + (sample_size - 1) * z_for_bpw(N, W, H, bpw, sample_size - 1, device)) / sample_size
+        return bpw, z
+
+    bpw1, z1 = search(guess, 31.0, 37.0, 34.0)
+    bpw2, z2 = search(bpw1 + (z1 - 22) * step, 20.0, 25.0, 21.0)
+    return bpw2 + (bpw1 - bpw2) * (target - z2) / (z1 - z2), (bpw1, z1), (bpw2, z2)
+
+
+def bpw_scan_z(shapes, device=0, verbose=True):
+    """The max-bpw table by the reference's criterion (round-off Z = 28): {N: (W, H, max_bpw, points)}."""
+    from gpuowl_b200 import build
+    build.build()
+    out = {}
+    for (N, W, H) in shapes:
+        import math
+        guess = 19.2 - 0.3 * (math.log2(N) - 18.0) - 0.2  # a little below the library's default limit
+        best, p1, p2 = max_bpw_z(N, W, H, guess, device, verbose=verbose)
+        out[N] = (W, H, best, [p1, p2])
+    return out
+
+
+def write_bpw_z(table, out_txt):
+    with open(out_txt, "w") as f:
+        f.write("# max bits/word at round-off Z = 28 (the reference's Tune::maxBpw criterion), "
+                "interpolated between a Z ~ 34 and a Z ~ 22 measurement\n")
+        f.write("# N  spec  max_bpw  (bpw:Z bpw:Z)\n")
+        for N in sorted(table):
+            W, H, best, pts = table[N]
+            f.write("%9d %14s %6.2f  %s\n" % (N, spec(W, H), best, " ".join("%.3f:%.2f" % p for p in pts)))
+
+
 def bpw_scan(shapes, iters, limit=0.3, start=16.0, step=0.25, device=0, verbose=True):
     """The reference's BPW table (src/fftbpw.h, measured by its -ztune) for this library's FFTs:
     for each (N, W, H) the largest bits per word, on a `step` grid from `start`, whose max round-off
@@ -198,7 +337,10 @@ def main():
     ap.add_argument("--json", default="tune.json")
     ap.add_argument("--five", action="store_true", help="also the 5 * 2^k FFT lengths")
     ap.add_argument("--bpw-scan", metavar="TUNE_JSON", help="measure the max bits/word of the shapes in TUNE_JSON")
-    ap.add_argument("--roe-limit", type=float, default=0.3)
+    ap.add_argument("--roe-limit", type=float, default=0.3,
+                    help="with --bpw-scan --criterion roe: the max round-off allowed")
+    ap.add_argument("--criterion", default="z", choices=["z", "roe"],
+                    help="with --bpw-scan: round-off Z = 28 (the reference's) or max round-off < --roe-limit")
     ap.add_argument("--shapes", metavar="WxH,...", help="per-pass times of these shapes (at 16 bits/word)")
     ap.add_argument("--split", action="store_true", help="with --shapes: the split-precision column pass")
     a = ap.parse_args()
@@ -211,8 +353,12 @@ def main():
             t = json.load(f)
         shapes = [(int(N), v[0], v[1]) for N, v in t.items()
                   if (1 << a.min_lg) <= int(N) <= (1 << a.max_lg)]
-        table = bpw_scan(sorted(shapes), a.iters, a.roe_limit)
-        write_bpw(table, a.roe_limit, a.iters, a.out)
+        if a.criterion == "z":
+            table = bpw_scan_z(sorted(shapes))
+            write_bpw_z(table, a.out)
+        else:
+            table = bpw_scan(sorted(shapes), a.iters, a.roe_limit)
+            write_bpw(table, a.roe_limit, a.iters, a.out)
         for N, (W, H, best, _) in table.items():
             if best and str(N) in t:
                 t[str(N)] = list(t[str(N)][:4]) + [best]

@@ -43,6 +43,15 @@ typedef struct {
   uint32_t proof_power;   /* power of the proof written (may be lower than asked when resuming without
                              the earlier residues, ProofSet::effectivePower), 0 = none */
   char proof_file[1024];  /* path of the verified proof file, "" = none */
+  /* round-off statistics (src/Gpu.cpp:1011-1025, src/Gpu.h:62-81): the per-squaring maximum
+     |x - rint(x)| of sampled blocks (the reference's wantROE sampling) fitted by a Gumbel law;
+     Z = (0.5 - miu) / beta says how many scale units the 0.5 failure point lies above the typical
+     maximum. The reference warns "Danger ROE!" when a log step's Z < 20. */
+  uint32_t roe_n;         /* sampled squarings over the whole run */
+  float roe_max;          /* their largest round-off */
+  float roe_z;            /* Z of the last log step's sample (0 = none) */
+  float roe_z_avg;        /* sample-size weighted mean Z over the run (the reference's zAvg) */
+  uint32_t n_danger_roe;  /* log steps whose Z fell below 20 */
 } owl_run_result;
 
 /* PRP-3 test of 2^E - 1 (src/Gpu.cpp:1400-1584): resumes from save_dir/<E>/ when a savefile exists. */

@@ -75,3 +75,25 @@ def test_large_shape_short_blocks_repeat(owl, oracle, E, W, H):
                 p.writeIn(a, w)
                 p.squareLoop(a, a, n)
                 assert np.array_equal(p.readOut(a), want[n]), (rep, n)
+
+
+def test_prp_roe_statistics_and_danger_warning(owl, oracle):
+    """Round-off statistics of the PRP loop (src/Gpu.cpp:1011-1025): sampled blocks give a Gumbel
+    Z per log step. At 16 bits per word on the 8K FFT the 0.5 failure point is far off (Z well
+    above 20, no warning); at 20.75 bits per word the same FFT runs close to it, Z drops and
+    every log step whose Z is below 20 is counted as a "Danger ROE" warning."""
+    N = 8192
+    lo = owl.prp_run(oracle.lib.oracle_next_prime(16 * N), W=64, H=64, block=500, log_step=1000,
+                     stop_after=3000)
+    assert lo["roe_n"] >= 1000 and lo["n_danger_roe"] == 0
+    assert lo["roe_z"] > 25 and lo["roe_max"] < 0.2
+    hi = owl.prp_run(oracle.lib.oracle_next_prime(int(20.75 * N)), W=64, H=64, block=500, log_step=1000,
+                     stop_after=3000)
+    assert hi["roe_n"] >= 1000 and hi["roe_z"] < lo["roe_z"] and hi["roe_max"] > lo["roe_max"]
+    if hi["roe_z_avg"] < 20:
+        assert hi["n_danger_roe"] >= 1
+
+
+def test_ll_roe_statistics(owl):
+    r = owl.ll_run(86243, log_step=10000, stop_after=20000)
+    assert r["roe_n"] >= 19000 and r["roe_z"] > 20 and r["n_danger_roe"] == 0
