@@ -225,36 +225,61 @@ def z_for_bpw(N, W, H, bpw, count=1, device=0, block=200, iters=2000, warmup=50)
     return total / count
 
 
+# the plan's limit on bits per word (owl_plan_create accepts E / N <= 21)
+BPW_CAP = 20.99
+
+
 def max_bpw_z(N, W, H, guess, device=0, target=28.0, sample_size=5, verbose=True):
     """Tune::maxBpw (src/tune.cpp:106-172): bits per word at which the round-off Z is `target` (28).
-    A secant search finds a bpw with Z in [31, 37] and one with Z in [20, 25], each re-measured on
+    A search finds a bpw with Z in [31, 37] and one with Z in [20, 25], each re-measured on
     `sample_size` exponents; the result interpolates between the two. `guess` is where the search
-    starts (the reference starts 9 steps below its table's value)."""
+    starts (the reference starts 9 steps below its table's value). The reference steps by a fixed
+    estimate of dbpw/dZ tuned at 4M-7.5M; here the step comes from the points measured so far (a
+    secant between the nearest points on either side of the band once it is bracketed), which also
+    holds for the small FFTs, where Z changes faster with bpw."""
     import math
-    step = 0.015 + (math.log2(N) - math.log2(4.0 * 1024 * 1024)) / \
+    step0 = 0.015 + (math.log2(N) - math.log2(4.0 * 1024 * 1024)) / \
         (math.log2(7.5 * 1024 * 1024) - math.log2(4.0 * 1024 * 1024)) * (0.012 - 0.015)
-    step = min(max(step, 0.005), 0.05)
+    step0 = min(max(step0, 0.005), 0.025)
+    seen = []
+
+    def z_at(bpw, count=1):
+        z = z_for_bpw(N, W, H, bpw, count, device)
+        if verbose:
+            print("N=%-9d %-14s bpw %.3f  Z %.2f%s" % (N, spec(W, H), bpw, z, " (x%d)" % count if count > 1 else ""),
+                  flush=True)
+        if count == 1:
+            seen.append((bpw, z))
+        return z
 
     def search(bpw, lo, hi, aim):
-        nonlocal step
-        z = z_for_bpw(N, W, H, bpw, 1, device)
-        if verbose:
-            print("N=%-9d %-14s bpw %.3f  Z %.2f" % (N, spec(W, H), bpw, z), flush=True)
-        for _ in range(40):
+        for _ in range(30):
+            bpw = min(max(bpw, 8.0), BPW_CAP)
+            z = z_at(bpw)
             if lo <= z <= hi:
                 break
-            prev_bpw, prev_z = bpw, z
-            bpw = bpw + (z - aim) * step
-            z = z_for_bpw(N, W, H, bpw, 1, device)
-            if verbose:
-                print("N=%-9d %-14s bpw %.3f  Z %.2f" % (N, spec(W, H), bpw, z), flush=True)
-            if z != prev_z:
-                step = min(max(-(bpw - prev_bpw) / (z - prev_z), 0.005), 0.025)
-        z = (z + (sample_size - 1) * z_for_bpw(N, W, H, bpw, sample_size - 1, device)) / sample_size
+            safe = [p for p in seen if p[1] > aim]    # Z above the aim: bpw can grow
+            risky = [p for p in seen if p[1] < aim]
+            if safe and risky:
+                a = max(safe)                          # the highest safe bpw
+                b = min(risky)                         # the lowest risky bpw
+                nxt = a[0] + (b[0] - a[0]) * (a[1] - aim) / (a[1] - b[1])
+            else:
+                # one side only: step by the local slope if two points exist, else by the default
+                pts = sorted(seen)[-2:] if safe else sorted(seen)[:2]
+                slope = (pts[1][0] - pts[0][0]) / (pts[0][1] - pts[1][1]) if len(pts) == 2 and pts[0][1] != pts[1][1] else 0
+                slope = slope if slope > 0 else step0
+                nxt = bpw + min(max((z - aim) * slope, -0.5), 0.5)
+            if z > hi and bpw >= BPW_CAP:
+                break                                  # safe up to the plan's limit
+            bpw = nxt
+        z = (z + (sample_size - 1) * z_at(bpw, sample_size - 1)) / sample_size
         return bpw, z
 
     bpw1, z1 = search(guess, 31.0, 37.0, 34.0)
-    bpw2, z2 = search(bpw1 + (z1 - 22) * step, 20.0, 25.0, 21.0)
+    bpw2, z2 = search(bpw1 + 0.1, 20.0, 25.0, 22.0)
+    if z1 == z2:
+        return bpw2, (bpw1, z1), (bpw2, z2)
     return bpw2 + (bpw1 - bpw2) * (target - z2) / (z1 - z2), (bpw1, z1), (bpw2, z2)
 
 
