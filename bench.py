@@ -156,6 +156,18 @@ def profiled_traffic():
     return {}
 
 
+def roe_measured(k, n):
+    """Whether the block of n squarings from iteration k measures its round-off. The reference's PRP
+    loop measures it on a sample only (src/Gpu.cpp:1026, 1459-1464: 2,000 iterations once the first
+    30 are past, then 400 after every 20,000-iteration log step; the other iterations run the kernel
+    build without it, src/Gpu.cpp:592-596), and so does owl_prp_run; a block is measured whole when
+    it holds a sampled iteration."""
+    if k < 2030 and k + n > 30:
+        return True
+    start = (k + n - 1) // 20000 * 20000  # the last log step before the block's end
+    return start >= 20000 and k < start + 400 and k + n > start
+
+
 def cpu_port_ms_per_iter(E, N, iters, threads):
     """The reference's IBDWT squaring restated on the CPU (oracle/ibdwt.c), ms per iteration."""
     import ctypes
@@ -271,15 +283,18 @@ def run_ours(args, rank, world, local):
         plan.writeIn(data, [3] + [0] * (plan.nwords - 1))
         plan.writeIn(check, [1] + [0] * (plan.nwords - 1))
         res = []
+        blk = [0]
 
         def step():
+            k = blk[0] * B
+            blk[0] += 1
             plan.modMul(check, data)
-            return plan.profile_square(data, B)
+            return plan.profile_square(data, B, roe=roe_measured(k, B))
 
         for _ in range(warmup):
             step()
             res.append("%016x" % plan.bufResidue(data))
-        plan.readROE()
+        roe_warm = plan.readROE()
         step_ms, prof = [], {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
         barrier()
         torch.cuda.synchronize()
@@ -299,7 +314,7 @@ def run_ours(args, rank, world, local):
                 res.append("%016x" % plan.bufResidue(data))
         torch.cuda.synchronize()
         barrier()
-        roe = plan.readROE()
+        roe = np.concatenate([roe_warm, plan.readROE()])
         # Gerbicz check of the final state (reference doCheck, src/Gpu.cpp:767-771)
         plan.squareLoop(aux, check, B, mul3=True)
         plan.modMul(check, data)
@@ -419,19 +434,49 @@ def run_ours(args, rank, world, local):
     return 0
 
 
+def _gmp_ms_per_iter(E, iters):
+    import ctypes
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+    lib.oracle_gmp_ms_per_iter.restype = ctypes.c_double
+    lib.oracle_gmp_ms_per_iter.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+    return lib.oracle_gmp_ms_per_iter(E, iters)
+
+
+def gmp_batch_baseline(exps, procs=8, iters=3):
+    """The CPU baseline of the batch: the GMP squaring loop (mod 2^E - 1) on `procs` processes of
+    one core each. Each exponent's ms per iteration is sampled (`iters` squarings after 40 warm-up
+    ones); a job of the same number of iterations for every exponent, spread evenly over the
+    processes, runs at procs * len(exps) / sum(seconds per iteration) aggregate iterations/s."""
+    import multiprocessing as mp
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True, capture_output=True)
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        ms = pool.starmap(_gmp_ms_per_iter, [(E, iters) for E in exps])
+    wall = time.perf_counter() - t0
+    rate = procs * len(exps) / (sum(ms) * 1e-3)
+    return {"value": round(rate, 1), "unit": "iter/s", "cores": procs, "kind": "port",
+            "sample": "GMP 6.3 mpz squaring mod 2^E-1 (oracle/gmp_loop.c, the exact oracle; the reference's "
+                      "OpenCL kernels have no CPU runtime here): %d squarings of each of the %d exponents after 40 "
+                      "warm-up ones, %d processes x 1 core, %.1f s wall; aggregate = %d x %d / sum of s/iter"
+                      % (iters, len(exps), procs, wall, procs, len(exps))}
+
+
 def run_batch64(args, rank, world, local):
     """64 exponents log-uniform in [1M, 20M] (seeded), each at the smallest FFT with <= 19 bits per
     word, squared together as one CUDA-graph launch per 1,000-iteration block; aggregate iter/s and
     per-exponent res64 at every 1,000 iterations against the GMP table."""
+    # the exponents and their res64 from the golden fixture (tests/golden/gen_golden.py batch64)
+    items = (load_golden("batch64") or {"items": []})["items"]
+    exps = [it["E"] for it in items]
+    golden = {it["E"]: it["res64"] for it in items}
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0:
+        cpu = gmp_batch_baseline(exps)
     import torch
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
     build.build()
     torch.cuda.set_device(local)
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    import gen_golden
-    exps = gen_golden.batch_exponents()
-    golden = {it["E"]: it["res64"] for it in (load_golden("batch64") or {"items": []})["items"]}
     B = args.block
     plans, bufs = [], []
     for E in exps:
@@ -443,24 +488,30 @@ def run_batch64(args, rank, world, local):
         bufs.append(b)
     batch = owl.Batch(plans, device=local)
     res = {E: [] for E in exps}
+    blk = [0]
 
-    def step():
-        batch.square(bufs, B)
+    def square():
+        # round-off measured on the reference's sample of iterations, as in the single-exponent line
+        batch.square(bufs, B, roe=roe_measured(blk[0] * B, B))
+        blk[0] += 1
         batch.sync()
-        for p, b in zip(plans, bufs):
-            res[p.E].append("%016x" % p.bufResidue(b))
 
     for _ in range(args.warmup):
-        step()
+        square()
+        for p, b in zip(plans, bufs):
+            res[p.E].append("%016x" % p.bufResidue(b))
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        batch.square(bufs, B)
-        batch.sync()
+        square()
         times.append(time.perf_counter() - t0)
         for p, b in zip(plans, bufs):
             res[p.E].append("%016x" % p.bufResidue(b))
     total = sum(times)
+    points = sum(p.N for p in plans)
+    groups = {}
+    for p in plans:
+        groups[(p.W, p.H)] = groups.get((p.W, p.H), 0) + 1
     checked = matched = 0
     for E in exps:
         g = golden.get(E, [])
@@ -474,8 +525,15 @@ def run_batch64(args, rank, world, local):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "64 exponents log-uniform in [1M,20M] (seed 20261203), FFT per exponent at <=19 "
                                    "bits/word, one graph launch per %d-iteration block" % B,
-                       "fft_sizes": shapes, "timing": "wall clock around launch + synchronize"},
-            "res64_checked": checked, "res64_matched": matched}
+                       "fft_sizes": shapes, "timing": "wall clock around launch + synchronize",
+                       "launches": "plans of one W x H shape (%d shapes) share one launch per pass: %d kernels per "
+                                   "iteration for the %d plans" % (len(groups), sum(2 * ((n + 15) // 16)
+                                                                                   for n in groups.values()),
+                                                                  len(plans))},
+            "res64_checked": checked, "res64_matched": matched,
+            "points_per_iteration": points,
+            "ns_per_mpoint_iter": round(1e9 * total / (args.steps * B) / (points / 1e6), 2),
+            "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     batch.close()
     for p in plans:
@@ -517,15 +575,18 @@ def run_prp_config(args, rank, world, local):
     plan.writeIn(check, [1] + [0] * (plan.nwords - 1))
     res, step_ms = [], []
     prof = {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
+    blk = [0]
 
     def step():
+        k = blk[0] * B
+        blk[0] += 1
         plan.modMul(check, data)
-        return plan.profile_square(data, B)
+        return plan.profile_square(data, B, roe=roe_measured(k, B))
 
     for _ in range(args.warmup):
         step()
         res.append("%016x" % plan.bufResidue(data))
-    plan.readROE()
+    roe_warm = plan.readROE()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
@@ -541,7 +602,8 @@ def run_prp_config(args, rank, world, local):
                 prof[k][0] += ms
                 prof[k][1] += n
             res.append("%016x" % plan.bufResidue(data))
-    roe = plan.readROE()
+    import numpy as np
+    roe = np.concatenate([roe_warm, plan.readROE()])
     plan.squareLoop(aux, check, B, mul3=True)
     plan.modMul(check, data)
     gerbicz_ok = plan.isEqual(check, aux)

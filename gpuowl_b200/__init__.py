@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(_HERE, "libowl.so")
 
 SQ_MUL3 = 1
 SQ_LL = 2
+SQ_NO_ROE = 4
 
 OK = 0
 ERR_TIMEOUT = -4
@@ -116,7 +117,8 @@ _SIGS = {
     "owl_batch_square": ([_P, ctypes.POINTER(_P), ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int),
     "owl_batch_sync": ([_P], ctypes.c_int),
     "owl_batch_destroy": ([_P], ctypes.c_int),
-    "owl_profile_square": ([_P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), _U32P], ctypes.c_int),
+    "owl_profile_square": ([_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float), _U32P],
+                           ctypes.c_int),
 }
 
 
@@ -267,8 +269,9 @@ class Plan:
         return w
 
     # -- engine ops --
-    def squareLoop(self, out, inp, n, mul3=False, ll=False):
-        flags = (SQ_MUL3 if mul3 else 0) | (SQ_LL if ll else 0)
+    def squareLoop(self, out, inp, n, mul3=False, ll=False, roe=True):
+        """n squarings; roe=False skips the round-off measurement (readROE gets no entries for them)."""
+        flags = (SQ_MUL3 if mul3 else 0) | (SQ_LL if ll else 0) | (0 if roe else SQ_NO_ROE)
         _check(self.lib.owl_square(self.h, out, inp, int(n), flags))
 
     def expMul(self, a, h, b):
@@ -308,11 +311,11 @@ class Plan:
         _check(self.lib.owl_plan_stream(self.h, ctypes.byref(s)))
         return s.value or 0
 
-    def profile_square(self, buf, n):
+    def profile_square(self, buf, n, roe=True):
         """Per-kernel device time of n squarings: {"pass2": (ms, launches), "pass1": ..., "edge": ...}."""
         ms = (ctypes.c_float * 3)()
         cnt = (ctypes.c_uint32 * 3)()
-        _check(self.lib.owl_profile_square(self.h, buf, int(n), ms, cnt))
+        _check(self.lib.owl_profile_square(self.h, buf, int(n), 0 if roe else SQ_NO_ROE, ms, cnt))
         return {"pass2": (ms[0], cnt[0]), "pass1": (ms[1], cnt[1]), "edge": (ms[2], cnt[2])}
 
     def probe_wait_timeout(self):
@@ -477,9 +480,9 @@ class Batch:
         _check(self.lib.owl_batch_create(device, len(self.plans), arr, ctypes.byref(h)))
         self.h = h
 
-    def square(self, bufs, n, ll=False):
+    def square(self, bufs, n, ll=False, roe=True):
         arr = (_P * len(bufs))(*bufs)
-        _check(self.lib.owl_batch_square(self.h, arr, int(n), SQ_LL if ll else 0))
+        _check(self.lib.owl_batch_square(self.h, arr, int(n), (SQ_LL if ll else 0) | (0 if roe else SQ_NO_ROE)))
 
     def sync(self):
         _check(self.lib.owl_batch_sync(self.h))

@@ -34,7 +34,7 @@ def sources():
     out = []
     for d in (CSRC, HOST):
         for name in sorted(os.listdir(d)):
-            if name.endswith((".cu", ".cuh", ".hpp", ".h", ".cpp")):
+            if name.endswith((".cu", ".cuh", ".inc", ".hpp", ".h", ".cpp")):
                 out.append(os.path.join(d, name))
     for name in sorted(os.listdir(INCLUDE)):
         out.append(os.path.join(INCLUDE, name))

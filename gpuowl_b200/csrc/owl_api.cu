@@ -134,12 +134,26 @@ template <int W, int M> void setp1attr() {
   size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
   ck(cudaFuncSetAttribute(owl::k_pass1<W, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
      "cudaFuncSetAttribute(pass1)");
+  ck(cudaFuncSetAttribute(owl::k_pass1_group<W, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+     "cudaFuncSetAttribute(pass1 group)");
+  if (M == owl::P1_FUSED) {
+    ck(cudaFuncSetAttribute(owl::k_pass1<W, kR, owl::P1_FUSED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sm),
+       "cudaFuncSetAttribute(pass1 without round-off)");
+    ck(cudaFuncSetAttribute(owl::k_pass1_group<W, kR, owl::P1_FUSED, false>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+       "cudaFuncSetAttribute(pass1 group without round-off)");
+  }
 }
 template <int H, int M> void setp2attr() {
   constexpr int V = owl::p2_vpt(H);
   size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
   ck(cudaFuncSetAttribute(owl::k_pass2<H, kR, M, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
      "cudaFuncSetAttribute(pass2)");
+  if (M == owl::P2_SQUARE) {
+    ck(cudaFuncSetAttribute(owl::k_pass2_group<H, kR, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+       "cudaFuncSetAttribute(pass2 group)");
+  }
 }
 
 template <int M> void setp2tcattr() {
@@ -151,23 +165,28 @@ template <int M> void setp2tcattr() {
 // kernel before it (the pass kernels begin with griddep_wait()): its CTAs may be scheduled on SMs
 // that the previous pass's last CTAs leave free, which hides the launch gap between the passes.
 template <typename... KArgs, typename... Args>
-void launch_pass(owl_plan* p, bool pdl, void (*kernel)(KArgs...), dim3 grid, int threads, size_t smem,
-                 Args... args) {
+void launch_on(cudaStream_t stream, bool pdl, void (*kernel)(KArgs...), dim3 grid, int threads, size_t smem,
+               Args... args) {
   if (!pdl) {
-    kernel<<<grid, threads, smem, p->stream>>>(args...);
+    kernel<<<grid, threads, smem, stream>>>(args...);
     return;
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = smem;
-  cfg.stream = p->stream;
+  cfg.stream = stream;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
   ck(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...), "cudaLaunchKernelEx");
+}
+template <typename... KArgs, typename... Args>
+void launch_pass(owl_plan* p, bool pdl, void (*kernel)(KArgs...), dim3 grid, int threads, size_t smem,
+                 Args... args) {
+  launch_on(p->stream, pdl, kernel, grid, threads, smem, args...);
 }
 
 void p2launch_tc(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
@@ -184,7 +203,9 @@ template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int 
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
   dim3 grid(p->H / kR);
-  auto k = (mode == owl::P1_FUSED) ? owl::k_pass1<W, kR, owl::P1_FUSED>
+  // a fused pass with no round-off slot runs the build without the measurement
+  auto k = (mode == owl::P1_FUSED) ? (roeSlot >= 0 ? owl::k_pass1<W, kR, owl::P1_FUSED>
+                                                   : owl::k_pass1<W, kR, owl::P1_FUSED, false>)
            : (mode == owl::P1_IN)  ? owl::k_pass1<W, kR, owl::P1_IN>
                                    : owl::k_pass1<W, kR, owl::P1_OUT>;
   launch_pass(p, pdl, k, grid, T, sm, p->args, F, words, roeSlot, flags, ts);
@@ -237,10 +258,12 @@ void set_attrs(uint32_t W, uint32_t H) {
   }
 }
 
+constexpr int kNoRoe = -2;  // pass1's fixedSlot for a line pass that measures no round-off
+
 void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot = -1, int ts = -1,
            bool pdl = false) {
   int slot = -1;
-  if (mode != owl::P1_IN) {
+  if (mode != owl::P1_IN && fixedSlot != kNoRoe) {
     if (fixedSlot >= 0) {
       slot = std::min(fixedSlot, (int)kRoeCap - 1);
       p->roePos = std::max(p->roePos, (uint32_t)slot + 1);
@@ -298,6 +321,7 @@ constexpr uint32_t kTsCap = 4096;  // launch-timestamp slots (profiled blocks of
 void enqueue_square(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags, bool stamp) {
   const int ll = (flags & OWL_SQ_LL) ? owl::FL_LL : 0;
   const int mul3 = (flags & OWL_SQ_MUL3) ? owl::FL_MUL3 : 0;
+  const bool roe = !(flags & OWL_SQ_NO_ROE);
   int li = 0;
   auto ts = [&] { return stamp ? li++ : -1; };
   if (stamp) {
@@ -312,11 +336,79 @@ void enqueue_square(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, ui
   for (uint32_t k = 0; k < n; ++k) {
     pass2(p, owl::P2_SQUARE, p->F1, nullptr, nullptr, ts(), true);
     if (k + 1 < n) {
-      pass1(p, owl::P1_FUSED, p->F1, nullptr, ll, (int)k, ts(), pdl);
+      pass1(p, owl::P1_FUSED, p->F1, nullptr, ll, roe ? (int)k : kNoRoe, ts(), pdl);
     } else {
-      pass1_out(p, out, ll | mul3, (int)k, ts(), pdl);
+      pass1_out(p, out, ll | mul3, roe ? (int)k : kNoRoe, ts(), pdl);
     }
   }
+}
+
+// ---- grouped launches: the same pass of several plans of one shape in one launch ----
+
+template <int W> void p1group(cudaStream_t st, int mode, bool roe, const owl::GroupArgs& ga, uint32_t cnt, uint32_t H,
+                              int roeSlot, int flags) {
+  constexpr int T = kR * W / 16;
+  const size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
+  const dim3 grid(H / kR, cnt);
+  auto k = (mode == owl::P1_FUSED) ? (roe ? owl::k_pass1_group<W, kR, owl::P1_FUSED>
+                                          : owl::k_pass1_group<W, kR, owl::P1_FUSED, false>)
+           : (mode == owl::P1_IN)  ? owl::k_pass1_group<W, kR, owl::P1_IN>
+                                   : owl::k_pass1_group<W, kR, owl::P1_OUT>;
+  launch_on(st, mode != owl::P1_IN, k, grid, T, sm, ga, roeSlot, flags);
+}
+template <int H> void p2group(cudaStream_t st, const owl::GroupArgs& ga, uint32_t cnt, uint32_t W) {
+  constexpr int V = owl::p2_vpt(H);
+  const size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
+  launch_on(st, true, owl::k_pass2_group<H, kR, V>, dim3(W / 2, cnt), 2 * H / V, sm, ga);
+}
+
+// n squarings of each plan's buffer (in place) as grouped launches on `st`: plans of one plain
+// (not split-precision) shape, at most kGroupMax
+void enqueue_square_group(cudaStream_t st, const std::vector<owl_plan*>& plans, const std::vector<int32_t*>& bufs,
+                          uint32_t n, uint32_t flags) {
+  const uint32_t cnt = (uint32_t)plans.size();
+  const uint32_t W = plans[0]->W, H = plans[0]->H;
+  owl::GroupArgs ga{};
+  for (uint32_t i = 0; i < cnt; ++i) {
+    ga.a[i] = plans[i]->args;
+    ga.F[i] = plans[i]->F1;
+    ga.words[i] = bufs[i];
+  }
+  const int ll = (flags & OWL_SQ_LL) ? owl::FL_LL : 0;
+  const int mul3 = (flags & OWL_SQ_MUL3) ? owl::FL_MUL3 : 0;
+  const bool roe = !(flags & OWL_SQ_NO_ROE);
+  auto p1 = [&](int mode, int slot, int fl) {
+    switch (W) {
+#define CASE_W(x)                                                   \
+  case x:                                                           \
+    p1group<x>(st, mode, slot >= 0, ga, cnt, H, slot, fl);          \
+    break;
+      OWL_FOR_SIZES(CASE_W)
+#undef CASE_W
+      default:
+        fail(OWL_ERR_ARG, "unsupported W");
+    }
+  };
+  auto p2 = [&]() {
+    switch (H) {
+#define CASE_H(x)                            \
+  case x:                                    \
+    p2group<x>(st, ga, cnt, W);              \
+    break;
+      OWL_FOR_H_SIZES(CASE_H)
+#undef CASE_H
+      default:
+        fail(OWL_ERR_ARG, "unsupported H");
+    }
+  };
+  p1(owl::P1_IN, -1, 0);
+  for (uint32_t k = 0; k < n; ++k) {
+    p2();
+    const int slot = roe ? (int)std::min(k, kRoeCap - 1) : -1;
+    p1(k + 1 < n ? owl::P1_FUSED : owl::P1_OUT, slot, k + 1 < n ? ll : (ll | mul3));
+  }
+  owl::k_carry_fixup_group<<<cnt, 32, 0, st>>>(ga);
+  ck(cudaGetLastError(), "grouped launch");
 }
 
 constexpr uint32_t kGraphMinIters = 16;
@@ -363,7 +455,7 @@ void run_square(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, uint32
   }
   auto& g = graph_for(p, out, in, n, flags, false);
   ck(cudaGraphLaunch(g.exec, p->stream), "cudaGraphLaunch");
-  p->roePos = std::max(p->roePos, std::min(n, kRoeCap));
+  if (!(flags & OWL_SQ_NO_ROE)) { p->roePos = std::max(p->roePos, std::min(n, kRoeCap)); }
 }
 
 void check_plan(const owl_plan* p) {
@@ -811,7 +903,7 @@ int owl_square(owl_plan* plan, int32_t* out, const int32_t* in, uint32_t n, uint
       return;
     }
     DeviceGuard dg(plan->device);
-    run_square(plan, out, in, n, flags & (OWL_SQ_LL | OWL_SQ_MUL3));
+    run_square(plan, out, in, n, flags & (OWL_SQ_LL | OWL_SQ_MUL3 | OWL_SQ_NO_ROE));
   });
 }
 
@@ -958,15 +1050,16 @@ int owl_plan_stream(owl_plan* plan, void** stream) {
   });
 }
 
-int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint32_t* launches) {
+int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, uint32_t flags, float* ms, uint32_t* launches) {
   return guarded([&] {
     check_plan(plan);
     check_buf(plan, buf);
     if (!ms || !launches || n == 0 || 2 * n + 1 > kTsCap) { fail(OWL_ERR_ARG, "bad argument"); }
     DeviceGuard dg(plan->device);
-    auto& g = graph_for(plan, buf, buf, n, 0, true);
+    flags &= OWL_SQ_LL | OWL_SQ_MUL3 | OWL_SQ_NO_ROE;
+    auto& g = graph_for(plan, buf, buf, n, flags, true);
     ck(cudaGraphLaunch(g.exec, plan->stream), "cudaGraphLaunch");
-    plan->roePos = std::max(plan->roePos, std::min(n, kRoeCap));
+    if (!(flags & OWL_SQ_NO_ROE)) { plan->roePos = std::max(plan->roePos, std::min(n, kRoeCap)); }
     const size_t cnt = 2 * (size_t)n + 1;
     std::vector<unsigned long long> t0(cnt), t1(cnt);
     ck(cudaMemcpyAsync(t0.data(), plan->args.tsStart, cnt * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -1027,15 +1120,48 @@ cudaGraphExec_t batch_graph(owl_batch* b, int32_t* const* bufs, uint32_t n, uint
     b->graphs.erase(b->graphs.begin());
   }
   cudaGraph_t graph = nullptr;
+  // plans of one plain shape run as grouped launches (one branch per group of up to kGroupMax, on
+  // its first plan's stream); split-precision plans and shapes of one plan get a branch each
+  std::vector<std::vector<size_t>> branches;
+  {
+    std::vector<std::pair<uint64_t, size_t>> order;
+    for (size_t i = 0; i < b->plans.size(); ++i) {
+      const owl_plan* p = b->plans[i];
+      const uint64_t key = p->split ? (1ull << 63) | i : ((uint64_t)p->W << 32) | p->H;
+      order.push_back({key, i});
+    }
+    std::stable_sort(order.begin(), order.end());
+    for (size_t i = 0; i < order.size();) {
+      size_t j = i;
+      std::vector<size_t> g;
+      while (j < order.size() && order[j].first == order[i].first && g.size() < (size_t)owl::kGroupMax) {
+        g.push_back(order[j].second);
+        ++j;
+      }
+      branches.push_back(g);
+      i = j;
+    }
+  }
   ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
   try {
     ck(cudaEventRecord(b->fork, b->stream), "fork");
-    for (size_t i = 0; i < b->plans.size(); ++i) {
-      owl_plan* p = b->plans[i];
+    for (size_t bi = 0; bi < branches.size(); ++bi) {
+      const auto& g = branches[bi];
+      owl_plan* p = b->plans[g[0]];
       ck(cudaStreamWaitEvent(p->stream, b->fork, 0), "fork wait");
-      enqueue_square(p, bufs[i], bufs[i], n, flags, false);
-      ck(cudaEventRecord(b->joins[i], p->stream), "join");
-      ck(cudaStreamWaitEvent(b->stream, b->joins[i], 0), "join wait");
+      if (g.size() == 1) {
+        enqueue_square(p, bufs[g[0]], bufs[g[0]], n, flags, false);
+      } else {
+        std::vector<owl_plan*> gp;
+        std::vector<int32_t*> gb;
+        for (size_t i : g) {
+          gp.push_back(b->plans[i]);
+          gb.push_back(bufs[i]);
+        }
+        enqueue_square_group(p->stream, gp, gb, n, flags);
+      }
+      ck(cudaEventRecord(b->joins[bi], p->stream), "join");
+      ck(cudaStreamWaitEvent(b->stream, b->joins[bi], 0), "join wait");
     }
   } catch (...) {
     cudaStreamEndCapture(b->stream, &graph);
@@ -1087,12 +1213,13 @@ int owl_batch_square(owl_batch* b, int32_t* const* bufs, uint32_t n, uint32_t fl
       ck(cudaEventRecord(b->joins[i], b->plans[i]->stream), "record");
       ck(cudaStreamWaitEvent(b->stream, b->joins[i], 0), "wait");
     }
-    cudaGraphExec_t exec = batch_graph(b, bufs, n, flags & (OWL_SQ_LL | OWL_SQ_MUL3));
+    flags &= OWL_SQ_LL | OWL_SQ_MUL3 | OWL_SQ_NO_ROE;
+    cudaGraphExec_t exec = batch_graph(b, bufs, n, flags);
     ck(cudaGraphLaunch(exec, b->stream), "cudaGraphLaunch");
     ck(cudaEventRecord(b->done, b->stream), "record");
     for (owl_plan* p : b->plans) {
       ck(cudaStreamWaitEvent(p->stream, b->done, 0), "wait");
-      p->roePos = std::max(p->roePos, std::min(n, kRoeCap));
+      if (!(flags & OWL_SQ_NO_ROE)) { p->roePos = std::max(p->roePos, std::min(n, kRoeCap)); }
     }
   });
 }

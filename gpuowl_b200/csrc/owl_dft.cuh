@@ -323,6 +323,13 @@ __host__ __device__ constexpr int p2_vpt(int H) {
   return (OWL_P2_VPT == 8 && (H & (H - 1)) == 0 && H <= 2048) ? 8 : 16;
 }
 
+// CTAs per SM that the pass kernels' launch bounds ask for: enough for 16 resident warps at most
+// 128 registers a thread (T threads a CTA; at most 32 CTAs an SM). Without the hint the kernels of
+// the small FFTs (32- to 128-thread CTAs) took 200-255 registers, which left 8-10 warps on an SM.
+constexpr int occ_blocks(int T) {
+  return T >= 512 ? 1 : (16 / ((T + 31) / 32) > 32 ? 32 : 16 / ((T + 31) / 32));
+}
+
 // Stage twiddle tables, one per stage with twiddles, each laid out [r][k]:
 // entry r * NS + k = w_(R NS)^(r k) (forward sign), so that a warp's threads
 // (consecutive k) read one contiguous run per r. Offsets in complex elements.

@@ -377,23 +377,23 @@ class HostGpu {
     copy(aux, check);
     uint32_t n = 1;
     for (; B % (2 * n) == 0; n *= 2) {
-      squareLoop(data, data, n);
+      squareLoop(data, data, n, OWL_SQ_NO_ROE);
       modMul(data, aux);
       copy(aux, data);
     }
     uint32_t blocks = B / n;
     if (blocks < 2) { fail(OWL_ERR_ARG, "block size must not be a power of two"); }
     for (uint32_t i = 0; i + 2 < blocks; ++i) {
-      squareLoop(data, data, n);
+      squareLoop(data, data, n, OWL_SQ_NO_ROE);
       modMul(data, aux);
     }
-    squareLoop(data, data, n);
+    squareLoop(data, data, n, OWL_SQ_NO_ROE);
     modMul(data, aux, true);
   }
 
   // src/Gpu.cpp:767-771
   bool doCheck(uint32_t B) {
-    squareLoop(aux, check, B, OWL_SQ_MUL3);
+    squareLoop(aux, check, B, OWL_SQ_MUL3 | OWL_SQ_NO_ROE);
     modMul(check, data);
     return isEqual(check, aux);
   }
@@ -413,7 +413,7 @@ class HostGpu {
     writeIn(data, A);
     for (uint32_t k = 0; k < n;) {
       const uint32_t its = std::min(1000u, n - k);
-      squareLoop(data, data, its);
+      squareLoop(data, data, its, OWL_SQ_NO_ROE);
       k += its;
     }
     return readOut(data);
@@ -750,9 +750,9 @@ struct RoeInfo {
   double z(double x = 0.5) const { return N && beta > 0 ? (x - miu) / beta : 0.0; }
 };
 
-// Which squaring blocks feed the statistics: the reference measures the round-off on a few
-// iterations only (wantROE, src/Gpu.cpp:1459-1464, 1026): 2,000 iterations once the first 30 of a
-// run are past, then 400 after every log step. Blocks are sampled whole here.
+// Which squarings feed the statistics: the reference measures the round-off on a few iterations
+// only (wantROE, src/Gpu.cpp:1459-1464, 1026): 2,000 iterations once the first 30 of a run are
+// past, then 400 after every log step; the other squarings run without the measurement.
 struct RoeSampler {
   uint32_t skipTo = 0;
   uint32_t want = 0;
@@ -762,7 +762,19 @@ struct RoeSampler {
     skipTo = startK + 30;
     want = 2000;
   }
-  bool takes(uint32_t k) const { return want > 0 && k >= skipTo; }
+  // n squarings from iteration k with `flags`: the ones the sample wants measure their round-off,
+  // the others run the kernels without the measurement (OWL_SQ_NO_ROE)
+  template <typename G> void square(G& gpu, int32_t* buf, uint32_t k, uint32_t n, uint32_t flags) {
+    const uint32_t skip = k < skipTo ? std::min(n, skipTo - k) : 0;
+    const uint32_t take = std::min(n - skip, want);
+    if (skip) { gpu.squareLoop(buf, buf, skip, flags | OWL_SQ_NO_ROE); }
+    if (take) {
+      gpu.readRoe();  // drops what other calls (the modMul) recorded
+      gpu.squareLoop(buf, buf, take, flags);
+      add(take, gpu.readRoe());
+    }
+    if (n - skip - take) { gpu.squareLoop(buf, buf, n - skip - take, flags | OWL_SQ_NO_ROE); }
+  }
   void add(uint32_t iters, std::vector<float> v) {
     want = iters >= want ? 0 : want - iters;
     sample.insert(sample.end(), v.begin(), v.end());
@@ -863,10 +875,7 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
       uint32_t next = roundUp(k + 1, B);
       if (k < kEnd && kEnd < next) { next = kEnd; }
       if (persistK > k && persistK < next) { next = persistK; }
-      const bool sample = roe.takes(k);
-      if (sample) { gpu.readRoe(); }  // drops what the modMul recorded
-      gpu.squareLoop(gpu.data, gpu.data, next - k);
-      if (sample) { roe.add(next - k, gpu.readRoe()); }
+      roe.square(gpu, gpu.data, k, next - k, 0);
       k = next;
       if (k == persistK) {
         proofSet->save(k, gpu.readOut(gpu.data));
@@ -966,20 +975,14 @@ void ll(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
     const uint32_t startK = k, kEnd = E - 2;
     bool reload = false;
     // round-off statistics per log step (the reference computes none in its LL loop, src/Gpu.cpp:1588;
-    // the same Z and danger warning as the PRP loop's are logged here)
+    // the same sampling, Z and danger warning as the PRP loop's are used here)
     RoeSampler roe;
+    roe.start(startK);
     while (true) {
       uint32_t next = roundUp(k + 1, logStep);
       if (next > kEnd) { next = kEnd; }
       if (o.stop_after && next - startK > o.stop_after) { next = std::max(k + 1, startK + o.stop_after); }
-      gpu.squareLoop(gpu.data, gpu.data, next - k, OWL_SQ_LL);
-      {
-        // slot i holds squaring i of this call; the first 30 of the run are left out, as in the PRP loop
-        std::vector<float> rv = gpu.readRoe();
-        const size_t skip = k - startK < 30 ? std::min<size_t>(30 - (k - startK), rv.size()) : 0;
-        rv.erase(rv.begin(), rv.begin() + skip);
-        roe.add(next - k, std::move(rv));
-      }
+      roe.square(gpu, gpu.data, k, next - k, OWL_SQ_LL);
       k = next;
       const bool doStop = (k >= kEnd) || (o.stop_after && k - startK >= o.stop_after);
       Words w = gpu.readOut(gpu.data);

@@ -45,6 +45,10 @@ enum {
 /* flags for owl_square */
 #define OWL_SQ_MUL3 1u /* multiply the result of the LAST squaring by 3 (src/Gpu.cpp:936-945 doTailMul3) */
 #define OWL_SQ_LL 2u   /* LL step x^2 - 2 on every squaring (src/Gpu.cpp:1586-1663, src/cl/carryfused.cl:120-123) */
+/* no round-off measurement in these squarings: the reference measures it on a sample of iterations
+   only (wantROE: 2,000 after the first 30, then 400 per log step, src/Gpu.cpp:1026, 1459-1464; the
+   kernel build without it, kCarryFused, src/Gpu.cpp:592-596); owl_read_roe gets no entries for them */
+#define OWL_SQ_NO_ROE 4u
 
 typedef struct owl_plan owl_plan;
 
@@ -100,7 +104,7 @@ int owl_read_words(owl_plan* plan, const int32_t* buf, uint32_t* words);
 
 /* Gpu::squareLoop(out, in, 0, n, flags & MUL3) (src/Gpu.cpp:936-945) with Gpu::square's
    kernel chain (src/Gpu.cpp:903-932): n squarings of `in` into `out` (out may equal in).
-   OWL_SQ_LL makes every step x^2 - 2 (squareLL). */
+   OWL_SQ_LL makes every step x^2 - 2 (squareLL); OWL_SQ_NO_ROE skips the round-off measurement. */
 int owl_square(owl_plan* plan, int32_t* out, const int32_t* in, uint32_t n, uint32_t flags);
 /* Gpu::modMul(ioA, inB, mul3) (src/Gpu.cpp:712-736): ioA := ioA * inB (* 3). */
 int owl_modmul(owl_plan* plan, int32_t* io_a, const int32_t* in_b, int mul3);
@@ -129,8 +133,9 @@ int owl_plan_stream(owl_plan* plan, void** stream);
    reference's -time profile (src/Gpu.cpp:773-799, src/Queue.cpp:54-58). The block runs as the
    same CUDA graph as owl_square; each kernel launch stamps its first CTA start and last CTA end
    with the GPU's global timer. ms[0] = total pass-2 (column) time, ms[1] = total pass-1
-   (line/carry) time, ms[2] = entry and exit passes; launches[0..2] the matching counts. */
-int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, float* ms, uint32_t* launches);
+   (line/carry) time, ms[2] = entry and exit passes; launches[0..2] the matching counts. flags as
+   for owl_square. */
+int owl_profile_square(owl_plan* plan, int32_t* buf, uint32_t n, uint32_t flags, float* ms, uint32_t* launches);
 
 /* Failure-detection probe: one device wait on a flag nothing sets, with the plan's
    timeout. Returns OWL_ERR_TIMEOUT (the expected outcome) and leaves the plan usable. */

@@ -8,7 +8,8 @@
 //   owl_emu pack E N pattern            (device expand / compact vs owl_words.hpp; prints "pack ok")
 //   owl_emu chain nblocks seed          (the block-carry chain vs its serial definition; "chain ok")
 // With OWL_EMU_SPLIT=1 in the environment and H = 2048 the column pass runs the
-// split-precision kernel (k_pass2_tc) on the emulated tensor cores.
+// split-precision kernel (k_pass2_tc) on the emulated tensor cores. With OWL_EMU_NO_ROE=1 the
+// fused line passes run the build without the round-off measurement.
 // Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
 #define OWL_EMU 1
 #include <algorithm>
@@ -103,6 +104,11 @@ template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * p1_line_stride<W, kR>() * sizeof(C);
   Args a = p.a;
+  if (M == P1_FUSED && std::getenv("OWL_EMU_NO_ROE")) {
+    // the build without the round-off measurement (OWL_SQ_NO_ROE)
+    emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M, false>(a, F, words, -1, flags, -1); });
+    return;
+  }
   emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M>(a, F, words, slot, flags, -1); });
 }
 template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {

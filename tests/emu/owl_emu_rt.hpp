@@ -29,6 +29,7 @@
 #define __host__
 #define __forceinline__ inline
 #define __launch_bounds__(...)
+#define __grid_constant__
 
 struct double2 {
   double x, y;

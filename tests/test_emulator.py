@@ -24,7 +24,7 @@ def emu():
     if shutil.which("g++") is None:
         pytest.skip("no g++")
     srcs = [os.path.join(EMU_DIR, f) for f in ("emu_main.cpp", "owl_emu_rt.hpp")] + \
-        [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp"))]
+        [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc", ".hpp"))]
     if not os.path.exists(EXE) or any(os.path.getmtime(s) > os.path.getmtime(EXE) for s in srcs):
         cmd = ["g++", "-std=c++20", "-O1", "-g", "-fsanitize=address", "-fno-omit-frame-pointer",
                "-DOWL_EMU", "-I", CSRC, "-I", EMU_DIR, "-o", EXE, os.path.join(EMU_DIR, "emu_main.cpp"),
@@ -129,3 +129,17 @@ def test_emulated_device_expand_compact(emu, E, N, pattern):
     r = subprocess.run([emu, "pack", str(E), str(N), str(pattern)], capture_output=True, text=True, timeout=600,
                        env=env)
     assert r.returncode == 0 and "pack ok" in r.stdout, (r.stdout[-500:], r.stderr[-2000:])
+
+
+@pytest.mark.parametrize("E,W,H,n,flags", [(86243, 64, 64, 40, 0), (500009, 128, 128, 24, 2)])
+def test_emulated_square_without_roe_matches_gmp(emu, oracle, E, W, H, n, flags):
+    """The fused line pass built without the round-off measurement (OWL_SQ_NO_ROE) gives the same
+    words."""
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", OWL_EMU_NO_ROE="1")
+    r = subprocess.run([emu, "square", str(E), str(W), str(H), str(n), str(flags), "0"], capture_output=True,
+                       text=True, timeout=900, env=env)
+    assert r.returncode == 0, r.stderr[-3000:]
+    got = np.array([int(x, 16) for x in r.stdout.strip().split("\n")[1].split()], dtype=np.uint32)
+    start = np.zeros((E - 1) // 32 + 1, dtype=np.uint32)
+    start[0] = 4 if flags & 2 else 3
+    assert np.array_equal(got, oracle.gmp_square(E, start, n, ll=bool(flags & 2)))

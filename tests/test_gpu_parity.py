@@ -68,6 +68,25 @@ def test_square_radix5_and_4k_shapes_vs_gmp(owl, oracle, E, W, H):
     assert roe < 0.3
 
 
+@pytest.mark.parametrize("E,W,H", [SHAPES[2], SHAPES[5], SHAPES[8], SHAPES_WIDE[0]])
+def test_square_without_roe(owl, oracle, E, W, H):
+    """OWL_SQ_NO_ROE: the line passes built without the round-off measurement give the same words
+    (GMP), record no round-off, and mix with measured blocks."""
+    n = 20
+    with owl.Plan(E, W=W, H=H) as p:
+        start = random_words(E, 7)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.readROE()
+        p.squareLoop(a, a, n, roe=False)
+        assert p.readROE().size == 0
+        p.squareLoop(a, a, n)
+        roe = p.readROE()
+        assert roe.size == n and 0 < roe.max() < 0.4
+        got = p.readOut(a)
+    assert np.array_equal(got, oracle.gmp_square(E, start, 2 * n))
+
+
 @pytest.mark.parametrize("E,W,H", [SHAPES[0], SHAPES[3], SHAPES[5], SHAPES[8]])
 def test_mul3_last(owl, oracle, E, W, H):
     """squareLoop with doTailMul3: the last squaring is multiplied by 3 (Gerbicz aux)."""
@@ -287,6 +306,61 @@ def test_batch64_golden(owl):
                     got[i].append("%016x" % p.bufResidue(b))
         for it, g in zip(golden["items"], got):
             assert g == it["res64"][:2], it["E"]
+    finally:
+        for p in plans:
+            p.close()
+
+
+def test_batch64_long_golden(owl):
+    """The 12 smallest exponents of the batch (64K and 80K FFTs: plans of one shape run as grouped
+    launches) for 10,000 iterations: res64 at every 1,000 equal the GMP golden table."""
+    golden = load_golden("batch64_long")
+    plans = []
+    for it in golden["items"]:
+        _, W, H = owl.fft_choose(it["E"], 19.0)
+        plans.append(owl.Plan(it["E"], W=W, H=H))
+    try:
+        bufs = []
+        for p in plans:
+            b = p.alloc()
+            p.writeIn(b, small_words(p.E, 3))
+            bufs.append(b)
+        got = [[] for _ in plans]
+        with owl.Batch(plans) as batch:
+            for blk in range(10):
+                batch.square(bufs, 1000, roe=blk < 2)
+                batch.sync()
+                for i, (p, b) in enumerate(zip(plans, bufs)):
+                    got[i].append("%016x" % p.bufResidue(b))
+        for it, g in zip(golden["items"], got):
+            assert g == it["res64"], it["E"]
+    finally:
+        for p in plans:
+            p.close()
+
+
+@pytest.mark.parametrize("ll", [False, True])
+def test_batch_grouped_launches_vs_gmp(owl, oracle, ll):
+    """Five plans of one shape (grouped launches) and one of another, squared together: each equals
+    GMP; the round-off is recorded per plan."""
+    exps = [86243, 86249, 100003, 110503, 120011]
+    plans = [owl.Plan(E, W=64, H=64) for E in exps] + [owl.Plan(500009, W=128, H=128)]
+    try:
+        bufs, starts = [], []
+        for p in plans:
+            b = p.alloc()
+            w = random_words(p.E, p.E ^ 0xBA7C)
+            p.writeIn(b, w)
+            bufs.append(b)
+            starts.append(w)
+            p.readROE()
+        with owl.Batch(plans) as batch:
+            batch.square(bufs, 30, ll=ll)
+            batch.sync()
+        for p, b, w in zip(plans, bufs, starts):
+            assert np.array_equal(p.readOut(b), oracle.gmp_square(p.E, w, 30, ll=ll)), p.E
+            roe = p.readROE()
+            assert roe.size == 30 and 0 < roe.max() < 0.3
     finally:
         for p in plans:
             p.close()

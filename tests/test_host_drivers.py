@@ -95,5 +95,7 @@ def test_prp_roe_statistics_and_danger_warning(owl, oracle):
 
 
 def test_ll_roe_statistics(owl):
+    """2,000 squarings sampled after the first 30, then 400 after the first log step."""
     r = owl.ll_run(86243, log_step=10000, stop_after=20000)
-    assert r["roe_n"] >= 19000 and r["roe_z"] > 20 and r["n_danger_roe"] == 0
+    assert r["finished"] is False and r["k"] == 20000
+    assert r["roe_n"] == 2400 and r["roe_z"] > 20 and r["n_danger_roe"] == 0
