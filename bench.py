@@ -358,8 +358,9 @@ def run_ours(args, rank, world, local):
         s_total, _, s_value = replica_summary(dist, split["total_ms"], 0.0, args.steps, B, world, device="cuda")
         sp = split["prof"]
         tc_ms = sp["pass2"][0] / max(sp["pass2"][1], 1)
-        # INT8 work of one k_pass2_tc launch: W/2 CTAs x 4 GEMM halves x 56 MMAs of 128 x 32 x 32
-        tc_ops = 2.0 * (W_8M // 2) * 4 * 56 * 128 * 32 * 32
+        # INT8 work of one k_pass2_tc launch: W/2 CTAs x 2 directions x 28 digit-plane products of a
+        # 128 x 64 (outputs) x 64 (inputs) GEMM (issued as 2 halves x 14 MMAs of N = 32 (7 - i))
+        tc_ops = 2.0 * (W_8M // 2) * 2 * 28 * 128 * 64 * 64
         bf16 = measured_bf16()
         split_line = {
             "form": "split-precision: 32-point column stages as INT8 tcgen05 GEMMs on 7 base-256 digit planes",

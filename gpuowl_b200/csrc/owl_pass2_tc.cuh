@@ -39,10 +39,17 @@ constexpr int kTcNHalf = 32;                    // N of one MMA batch
 constexpr int kTcASlice = kTcRows * kTcK;       // bytes of one data digit plane (8 KiB)
 constexpr int kTcBSlice = kTcN * kTcK;          // bytes of one DFT digit plane (4 KiB)
 constexpr int kTcBBytes = kTcSlices * kTcBSlice;
+// The DFT digit planes are stored per N half: the 32 output rows of the half, plane after plane,
+// as one K-major operand of 7 x 32 = 224 rows (row q = 32 j + n for plane j, output row n of the
+// half). One MMA then multiplies data plane i by planes 0 .. 6-i at once (N = 32 (7 - i)), and its
+// output column 32 (i + j) + n is accumulator d = i + j: each data plane is read once per k-step
+// instead of once per diagonal.
+constexpr int kTcBRows = kTcSlices * kTcNHalf;  // 224
+constexpr int kTcBHalf = kTcBRows * kTcK;       // bytes of one half's operand (14 KiB)
 constexpr uint32_t kTcTmemCols = 256;           // 7 accumulators x 32 columns, rounded to a power of two
 constexpr long long kTcBias = 0x0000808080808080LL;  // 128 in each of the 6 low digit positions
 // canonical-layout strides (bytes): K chunk stride = LBO, 8-row group stride = SBO = 128
-constexpr uint32_t kTcALbo = kTcRows * 16, kTcBLbo = kTcN * 16;
+constexpr uint32_t kTcALbo = kTcRows * 16, kTcBLbo = kTcBRows * 16;
 
 // dynamic shared memory: two column buffers (the data digit planes overlay
 // them), the DFT digit planes, row exponents, the MMA barrier, the TMEM base
@@ -53,11 +60,16 @@ constexpr int kTcOffBar = kTcOffExp + kTcRows * 4;
 constexpr int kTcOffTaddr = kTcOffBar + 8;
 constexpr int kTcSmem = kTcOffTaddr + 8;
 static_assert(kTcSlices * kTcASlice <= kTcOffB, "data digit planes must fit in the column buffers");
+static_assert(kTcBBytes == 2 * kTcBHalf, "DFT digit planes: two N halves");
 static_assert(kTcOffB % 16 == 0 && kTcOffBar % 8 == 0, "alignment");
 
 // byte offset of digit plane s, row `row`, K index kb in a canonical K-major operand of `rows` rows
 __host__ __device__ constexpr uint32_t tc_off(int rows, int s, int row, int kb) {
   return (uint32_t)(s * rows * 64 + (kb / 16) * rows * 16 + (row / 8) * 128 + (row % 8) * 16 + kb % 16);
+}
+// byte offset of DFT digit plane s, output row n (< 64), K index kb in the per-half operands
+__host__ __device__ constexpr uint32_t tc_off_b(int s, int n, int kb) {
+  return (uint32_t)((n / kTcNHalf) * kTcBHalf + tc_off(kTcBRows, 0, s * kTcNHalf + n % kTcNHalf, kb));
 }
 
 // the 7 digits of one value v (|v| < 2^54 after scaling), byte p of Z = Y + bias is digit 6 - p
@@ -97,21 +109,18 @@ __device__ __forceinline__ void tc_put_digits(unsigned char* sA, int row, int hh
   }
 }
 
-// issues the 56 MMAs of one N half: accumulator d (TMEM columns 32 d ..) gets sum_{i+j=d} A_i B_j^T
+// issues the 14 MMAs of one N half: accumulator d (TMEM columns 32 d ..) gets sum_{i+j=d} A_i B_j^T.
+// MMA (ks, i) multiplies data plane i by DFT planes 0 .. 6-i (N = 32 (7 - i)) into columns 32 i ..;
+// the first one (ks = 0, i = 0) covers all 7 accumulators and initialises them.
 __device__ __forceinline__ void tc_issue(uint32_t aBase, uint32_t bBase, uint32_t taddr, int half) {
-  constexpr uint32_t idesc = tc::idesc_s8(kTcRows, kTcNHalf);
 #pragma unroll
-  for (int d = 0; d < kTcSlices; ++d) {
+  for (int ks = 0; ks < kTcK / 32; ++ks) {
+    const uint64_t bd = tc::smem_desc(bBase + half * kTcBHalf + ks * 2 * kTcBLbo, kTcBLbo, 128);
 #pragma unroll
-    for (int i = 0; i <= d; ++i) {
-      const int j = d - i;
-#pragma unroll
-      for (int ks = 0; ks < kTcK / 32; ++ks) {
-        const uint64_t ad = tc::smem_desc(aBase + i * kTcASlice + ks * 2 * kTcALbo, kTcALbo, 128);
-        const uint64_t bd = tc::smem_desc(bBase + j * kTcBSlice + ks * 2 * kTcBLbo + half * (kTcNHalf / 8) * 128,
-                                          kTcBLbo, 128);
-        tc::mma_s8(taddr + (uint32_t)(d * kTcNHalf), ad, bd, idesc, i > 0 || ks > 0);
-      }
+    for (int i = 0; i < kTcSlices; ++i) {
+      const uint64_t ad = tc::smem_desc(aBase + i * kTcASlice + ks * 2 * kTcALbo, kTcALbo, 128);
+      tc::mma_s8(taddr + (uint32_t)(i * kTcNHalf), ad, bd, tc::idesc_s8(kTcRows, kTcNHalf * (kTcSlices - i)),
+                 i > 0 || ks > 0);
     }
   }
 }
@@ -398,8 +407,8 @@ static __global__ void k_tc_wait_probe(Args a) {
 
 namespace owl {
 
-// Host: the 7 digit planes of the 32-point DFT matrix in the canonical K-major
-// layout (64 output rows n = 2 m + {re, im}, 64 inputs kb = 2 r + {re, im}),
+// Host: the 7 digit planes of the 32-point DFT matrix in the per-half canonical K-major
+// layout of tc_off_b (64 output rows n = 2 m + {re, im}, 64 inputs kb = 2 r + {re, im}),
 // entries cos / sin of 2 pi r m / 32 scaled by 2^54 and rounded once.
 inline std::vector<uint8_t> tc_dft_digits() {
   std::vector<uint8_t> out(kTcBBytes);
@@ -414,7 +423,7 @@ inline std::vector<uint8_t> tc_dft_digits() {
       for (int p = 0; p < 7; ++p) {
         uint8_t b = (uint8_t)((unsigned long long)Z >> (8 * p));
         if (p < 6) { b ^= 0x80; }
-        out[tc_off(kTcN, 6 - p, n, kb)] = b;
+        out[tc_off_b(6 - p, n, kb)] = b;
       }
     }
   }
