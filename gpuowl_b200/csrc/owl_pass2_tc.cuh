@@ -48,28 +48,34 @@ constexpr int kTcBRows = kTcSlices * kTcNHalf;  // 224
 constexpr int kTcBHalf = kTcBRows * kTcK;       // bytes of one half's operand (14 KiB)
 constexpr uint32_t kTcTmemCols = 256;           // 7 accumulators x 32 columns, rounded to a power of two
 constexpr long long kTcBias = 0x0000808080808080LL;  // 128 in each of the 6 low digit positions
-// canonical-layout strides (bytes): K chunk stride = LBO, 8-row group stride = SBO = 128
-constexpr uint32_t kTcALbo = kTcRows * 16, kTcBLbo = kTcBRows * 16;
+// Both operands are K-major with 64-byte rows (the 64 int8 inputs of a GEMM row) in the 64-byte
+// swizzled layout (tc::sw64_off: 512-byte atoms of 8 rows, SBO = 512; one MMA's K = 32 bytes stays
+// inside a row, so LBO is unused); a k-step starts 32 bytes into the rows.
+constexpr uint32_t kTcSbo = 512;
 
 // dynamic shared memory: two column buffers (the data digit planes overlay
-// them), the DFT digit planes, row exponents, the MMA barrier, the TMEM base
+// them), the DFT digit planes, row exponents, the MMA barrier, the TMEM base;
+// the two operands start 1024-byte aligned (the swizzle is on address bits 4-8),
+// which the kernel arranges at run time inside the 1 KiB of slack (kTcAlign)
+constexpr int kTcAlign = 1024;
 constexpr int kTcColStride = p2_col_stride<kTcH>();
-constexpr int kTcOffB = 2 * kTcColStride * (int)sizeof(C);
+constexpr int kTcOffB = (2 * kTcColStride * (int)sizeof(C) + kTcAlign - 1) / kTcAlign * kTcAlign;
 constexpr int kTcOffExp = kTcOffB + kTcBBytes;
 constexpr int kTcOffBar = kTcOffExp + kTcRows * 4;
 constexpr int kTcOffTaddr = kTcOffBar + 8;
-constexpr int kTcSmem = kTcOffTaddr + 8;
+constexpr int kTcSmem = kTcOffTaddr + 8 + kTcAlign;
 static_assert(kTcSlices * kTcASlice <= kTcOffB, "data digit planes must fit in the column buffers");
+static_assert(kTcASlice % kTcAlign == 0 && kTcBHalf % kTcAlign == 0, "operand planes keep the swizzle alignment");
 static_assert(kTcBBytes == 2 * kTcBHalf, "DFT digit planes: two N halves");
 static_assert(kTcOffB % 16 == 0 && kTcOffBar % 8 == 0, "alignment");
 
-// byte offset of digit plane s, row `row`, K index kb in a canonical K-major operand of `rows` rows
-__host__ __device__ constexpr uint32_t tc_off(int rows, int s, int row, int kb) {
-  return (uint32_t)(s * rows * 64 + (kb / 16) * rows * 16 + (row / 8) * 128 + (row % 8) * 16 + kb % 16);
+// byte offset of data digit plane s, GEMM row `row`, K index kb
+__host__ __device__ constexpr uint32_t tc_off_a(int s, int row, int kb) {
+  return (uint32_t)(s * kTcASlice) + tc::sw64_off(row, kb);
 }
 // byte offset of DFT digit plane s, output row n (< 64), K index kb in the per-half operands
 __host__ __device__ constexpr uint32_t tc_off_b(int s, int n, int kb) {
-  return (uint32_t)((n / kTcNHalf) * kTcBHalf + tc_off(kTcBRows, 0, s * kTcNHalf + n % kTcNHalf, kb));
+  return (uint32_t)((n / kTcNHalf) * kTcBHalf) + tc::sw64_off(s * kTcNHalf + n % kTcNHalf, kb);
 }
 
 // the 7 digits of one value v (|v| < 2^54 after scaling), byte p of Z = Y + bias is digit 6 - p
@@ -104,7 +110,7 @@ __device__ __forceinline__ void tc_put_digits(unsigned char* sA, int row, int hh
     const int q = 2 * hh + qq;
 #pragma unroll
     for (int s = 0; s < kTcSlices; ++s) {
-      *reinterpret_cast<uint4*>(sA + tc_off(kTcRows, s, row, 16 * q)) = make_uint4(wd[s][0], wd[s][1], wd[s][2], wd[s][3]);
+      *reinterpret_cast<uint4*>(sA + tc_off_a(s, row, 16 * q)) = make_uint4(wd[s][0], wd[s][1], wd[s][2], wd[s][3]);
     }
   }
 }
@@ -115,10 +121,10 @@ __device__ __forceinline__ void tc_put_digits(unsigned char* sA, int row, int hh
 __device__ __forceinline__ void tc_issue(uint32_t aBase, uint32_t bBase, uint32_t taddr, int half) {
 #pragma unroll
   for (int ks = 0; ks < kTcK / 32; ++ks) {
-    const uint64_t bd = tc::smem_desc(bBase + half * kTcBHalf + ks * 2 * kTcBLbo, kTcBLbo, 128);
+    const uint64_t bd = tc::smem_desc(bBase + half * kTcBHalf + ks * 32, 16, kTcSbo, 4);
 #pragma unroll
     for (int i = 0; i < kTcSlices; ++i) {
-      const uint64_t ad = tc::smem_desc(aBase + i * kTcASlice + ks * 2 * kTcALbo, kTcALbo, 128);
+      const uint64_t ad = tc::smem_desc(aBase + i * kTcASlice + ks * 32, 16, kTcSbo, 4);
       tc::mma_s8(taddr + (uint32_t)(i * kTcNHalf), ad, bd, tc::idesc_s8(kTcRows, kTcNHalf * (kTcSlices - i)),
                  i > 0 || ks > 0);
     }
@@ -213,11 +219,14 @@ __global__ void __launch_bounds__(kTcH / 8, 2)
   constexpr int CS = kTcColStride;
   OWL_DYN_SHARED(C, smem);
   unsigned char* sm8 = reinterpret_cast<unsigned char*>(smem);
-  unsigned char* sA = sm8;
-  unsigned char* sB = sm8 + kTcOffB;
-  int* sExp = reinterpret_cast<int*>(sm8 + kTcOffExp);
-  uint64_t* sBar = reinterpret_cast<uint64_t*>(sm8 + kTcOffBar);
-  uint32_t* sTaddr = reinterpret_cast<uint32_t*>(sm8 + kTcOffTaddr);
+  // the operands 1024-byte aligned: the data planes overlay the column buffers from the first
+  // aligned address; everything from the DFT planes on moves by the same amount
+  const uint32_t alignPad = (uint32_t)(kTcAlign - (tc::smem_addr(sm8) & (kTcAlign - 1))) & (kTcAlign - 1);
+  unsigned char* sA = sm8 + alignPad;
+  unsigned char* sB = sm8 + alignPad + kTcOffB;
+  int* sExp = reinterpret_cast<int*>(sm8 + alignPad + kTcOffExp);
+  uint64_t* sBar = reinterpret_cast<uint64_t*>(sm8 + alignPad + kTcOffBar);
+  uint32_t* sTaddr = reinterpret_cast<uint32_t*>(sm8 + alignPad + kTcOffTaddr);
 
   const uint32_t W = a.W;
   const uint32_t c = blockIdx.x;
@@ -407,7 +416,7 @@ static __global__ void k_tc_wait_probe(Args a) {
 
 namespace owl {
 
-// Host: the 7 digit planes of the 32-point DFT matrix in the per-half canonical K-major
+// Host: the 7 digit planes of the 32-point DFT matrix in the per-half swizzled K-major
 // layout of tc_off_b (64 output rows n = 2 m + {re, im}, 64 inputs kb = 2 r + {re, im}),
 // entries cos / sin of 2 pi r m / 32 scaled by 2^54 and rounded once.
 inline std::vector<uint8_t> tc_dft_digits() {

@@ -3,10 +3,9 @@
 // both operands in shared memory, its completion barrier and the tensor-memory
 // reads of the INT32 accumulators.
 //
-// Shared-memory operands use the no-swizzle K-major canonical layout: a "core
-// matrix" is 8 rows x 16 bytes stored as 128 contiguous bytes (row r at byte
-// 16 r); core matrices adjacent along M/N are SBO bytes apart, the two along K
-// that one MMA (K = 32 bytes) reads are LBO bytes apart.
+// Shared-memory operands are K-major; smem_desc describes either the no-swizzle canonical layout (a
+// "core matrix" of 8 rows x 16 bytes stored as 128 contiguous bytes, core matrices SBO bytes apart
+// along M/N and LBO bytes apart along K) or the 64-byte swizzled one (sw64_off).
 //
 // With -DOWL_EMU (the CPU kernel emulator in tests/emu) the same calls run on
 // an emulated per-CTA tensor memory, and the MMA decodes its descriptors with
@@ -30,10 +29,15 @@ constexpr uint32_t idesc_s8(int M, int N) {
          | ((uint32_t)(M >> 4) << 24);  // M / 16
 }
 
-// shared-memory matrix descriptor, no swizzle, sm100 version field = 1
-__host__ __device__ constexpr uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// shared-memory matrix descriptor, sm100 version field = 1; layout 0 = no swizzle, 4 = 64-byte swizzle
+__host__ __device__ constexpr uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout = 0) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
+}
+// 64-byte swizzle of a K-major operand with 64-byte rows in 512-byte atoms of 8 rows (the atom
+// 1024-byte aligned): the 16-byte chunk c of row r is stored at chunk c ^ ((r % 8) / 2)
+__host__ __device__ constexpr uint32_t sw64_off(int row, int kb) {
+  return (uint32_t)((row / 8) * 512 + (row % 8) * 64 + (((kb / 16) ^ ((row % 8) >> 1)) * 16) + kb % 16);
 }
 
 __device__ __forceinline__ double exp2i(int k) { return __longlong_as_double((long long)(1023 + k) << 52); }
@@ -149,15 +153,28 @@ inline void mma_s8(uint32_t taddr, uint64_t adesc, uint64_t bdesc, uint32_t ides
   }
   const int M = (int)(((idesc >> 24) & 31u) << 4), N = (int)(((idesc >> 17) & 63u) << 3);
   auto decode = [&](uint64_t d, int rows, const char* what) {
-    if (((d >> 46) & 3u) != 1u || (d >> 61) != 0u || ((d >> 49) & 7u) != 0u) {
+    const uint32_t layout = (uint32_t)(d >> 61);
+    if (((d >> 46) & 3u) != 1u || (layout != 0u && layout != 4u) || ((d >> 49) & 7u) != 0u) {
       throw std::runtime_error(std::string("emu: bad descriptor ") + what);
     }
     const uint32_t start = (uint32_t)(d & 0x3FFFu) << 4, lbo = (uint32_t)((d >> 16) & 0x3FFFu) << 4,
                    sbo = (uint32_t)((d >> 32) & 0x3FFFu) << 4;
-    const size_t last = (size_t)start + (size_t)(rows / 8 - 1) * sbo + lbo + 127;
+    if (layout == 4u && (sbo != 512u || ((start & 1023u) & ~63u) != 0u)) {
+      throw std::runtime_error(std::string("emu: 64-byte swizzle needs 512-byte atoms at an aligned base ") + what);
+    }
+    const size_t last = layout == 4u ? (size_t)start + (size_t)(rows / 8 - 1) * sbo + 511
+                                     : (size_t)start + (size_t)(rows / 8 - 1) * sbo + lbo + 127;
     if (last >= c->dyn.size()) { throw std::runtime_error(std::string("emu: descriptor past smem ") + what); }
     return [=](int row, int k) -> int8_t {
-      size_t off = start + (size_t)(row / 8) * sbo + (size_t)(row % 8) * 16 + (size_t)(k / 16) * lbo + (k % 16);
+      size_t off;
+      if (layout == 4u) {
+        // rows of 64 bytes; the start may point inside the row (a later k-step); the XOR of the
+        // 16-byte chunk index with address bits 7-8 applies to the absolute address
+        off = start + (size_t)(row / 8) * sbo + (size_t)(row % 8) * 64 + (size_t)k;
+        off ^= ((off >> 7) & 3u) << 4;
+      } else {
+        off = start + (size_t)(row / 8) * sbo + (size_t)(row % 8) * 16 + (size_t)(k / 16) * lbo + (k % 16);
+      }
       return static_cast<int8_t>(c->dyn[off]);
     };
   };

@@ -97,6 +97,19 @@ int ref_proofset_save(const char* dir, uint32_t E, uint32_t power, uint32_t k, c
   }
 }
 
+// the reference's ProofSet::load of the residue at proof point k (CRC checked); 0 ok, -1 error
+int ref_proofset_load(const char* dir, uint32_t E, uint32_t power, uint32_t k, uint32_t* out) {
+  try {
+    if (!ProofSet::isInPoints(E, power, k)) { return -1; }
+    Cwd cwd{dir};
+    const Words w = ProofSet::load(E, power, k);
+    for (size_t i = 0; i < w.size(); ++i) { out[i] = w[i]; }
+    return 0;
+  } catch (...) {
+    return -1;
+  }
+}
+
 // the reference's ProofSet::computeProof from the residues under `dir`/<E>/proof/, then
 // Proof::save into `dir`; the file name goes to `outPath` (capacity `cap`)
 int ref_proof_compute_and_save(const char* dir, uint32_t E, uint32_t power, char* outPath, size_t cap) {
