@@ -763,8 +763,24 @@ struct RoeSampler {
     want = 2000;
   }
   // n squarings from iteration k with `flags`: the ones the sample wants measure their round-off,
-  // the others run the kernels without the measurement (OWL_SQ_NO_ROE)
-  template <typename G> void square(G& gpu, int32_t* buf, uint32_t k, uint32_t n, uint32_t flags) {
+  // the others run the kernels without the measurement (OWL_SQ_NO_ROE). With `whole`, a call the
+  // sample reaches is measured whole (the PRP loop's calls are blocks of B squarings: this keeps the
+  // number of distinct squaring graphs a plan caches small); its first squarings before skipTo are
+  // left out of the sample.
+  template <typename G> void square(G& gpu, int32_t* buf, uint32_t k, uint32_t n, uint32_t flags, bool whole = false) {
+    if (whole) {
+      if (want > 0 && k + n > skipTo) {
+        gpu.readRoe();  // drops what other calls (the modMul) recorded
+        gpu.squareLoop(buf, buf, n, flags);
+        std::vector<float> v = gpu.readRoe();
+        const size_t drop = k < skipTo ? std::min<size_t>(skipTo - k, v.size()) : 0;
+        v.erase(v.begin(), v.begin() + drop);
+        add(n, std::move(v));
+      } else {
+        gpu.squareLoop(buf, buf, n, flags | OWL_SQ_NO_ROE);
+      }
+      return;
+    }
     const uint32_t skip = k < skipTo ? std::min(n, skipTo - k) : 0;
     const uint32_t take = std::min(n - skip, want);
     if (skip) { gpu.squareLoop(buf, buf, skip, flags | OWL_SQ_NO_ROE); }
@@ -875,7 +891,7 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
       uint32_t next = roundUp(k + 1, B);
       if (k < kEnd && kEnd < next) { next = kEnd; }
       if (persistK > k && persistK < next) { next = persistK; }
-      roe.square(gpu, gpu.data, k, next - k, 0);
+      roe.square(gpu, gpu.data, k, next - k, 0, true);
       k = next;
       if (k == persistK) {
         proofSet->save(k, gpu.readOut(gpu.data));
