@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--block", type=int, default=BLOCK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tensor-core) form")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="prp8m on one GPU: skip the short runs of the other configurations (20M, 256K, "
+                         "batch64) whose lines the 8M line carries under \"configs\"")
     ap.add_argument("--workload", default="prp8m", choices=["prp8m", "batch64", "prp20m", "prp256k"],
                     help="prp8m: the headline line; batch64: 64 uneven exponents in one graph per block; "
                          "prp20m / prp256k: PRP-3 at the 20M FFT (5 * 2^22) / the 256K FFT")
@@ -433,6 +436,8 @@ def run_ours(args, rank, world, local):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
     }
+    if world == 1 and not args.no_configs:
+        line["configs"] = other_configs(args, rank, world, local)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -539,11 +544,10 @@ def run_batch64(args, rank, world, local):
             "points_per_iteration": points,
             "ns_per_mpoint_iter": round(1e9 * total / (args.steps * B) / (points / 1e6), 2),
             "cpu_baseline": cpu}
-    print(json.dumps(line), flush=True)
     batch.close()
     for p in plans:
         p.close()
-    return 0
+    return line
 
 
 # the other PRP configurations: golden table, shape (0 = the library's choice), range of E
@@ -620,7 +624,7 @@ def run_prp_config(args, rank, world, local):
     achieved = 16 * N / (avg_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
     if rank != 0:
-        return 0
+        return None
     line = {
         "metric": "ms/iter PRP @%s FFT, bit-exact res64" % label,
         "value": round(total_ms / (args.steps * B), 5), "unit": "ms/iter", "n_gpus": 1, "steps": args.steps,
@@ -641,17 +645,36 @@ def run_prp_config(args, rank, world, local):
         "gpu_launches": (2 * B + 8) * args.steps,
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
+
+
+# the short runs of the other configurations carried by the default (8M, one GPU) line:
+# (workload, timed steps, warm-up steps); each is the same code path as --workload <name>
+SUB_CONFIGS = (("prp20m", 2, 3), ("prp256k", 5, 3), ("batch64", 3, 3))
+
+
+def other_configs(args, rank, world, local):
+    """The lines of the 20M, 256K and batched configurations, each from a short run of its own
+    workload (a few 1,000-iteration blocks, res64 against its golden table), so that one default
+    run measures every configuration."""
+    out = {}
+    for name, steps, warmup in SUB_CONFIGS:
+        sub = argparse.Namespace(**vars(args))
+        sub.workload, sub.steps, sub.warmup = name, steps, warmup
+        run = run_batch64 if name == "batch64" else run_prp_config
+        out[name] = run(sub, rank, world, local)
+    return out
 
 
 def main():
     args = parse()
     rank, world, local = dist_env()
-    if args.workload == "batch64":
-        return run_batch64(args, rank, world, local)
-    if args.workload in PRP_CONFIGS:
-        return run_prp_config(args, rank, world, local)
+    if args.workload == "batch64" or args.workload in PRP_CONFIGS:
+        run = run_batch64 if args.workload == "batch64" else run_prp_config
+        line = run(args, rank, world, local)
+        if line is not None and rank == 0:
+            print(json.dumps(line), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_ours(args, rank, world, local)

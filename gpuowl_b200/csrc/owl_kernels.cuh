@@ -42,7 +42,7 @@ struct Args {
   double scaleLo;      // 2^bitsLo
   double iscaleLo;     // 2^-bitsLo
   const C* twW;    // stage tables of the width FFT (tw_offsets(W, 16/R) layout)
-  const C* twH;    // stage tables of the height FFT (tw_offsets(H, 8) layout)
+  const C* twH;    // stage tables of the height FFT (tw_offsets(H, p2_vpt(H) / 2, 0, p2_vpt(H)) layout)
   const C* rootH;  // w_H^i, i < H
   const C* twLo;   // w_hN^i, i < 2^loShift
   const C* twHi;   // w_hN^(i << loShift)

@@ -69,7 +69,8 @@ struct Layout {
 };
 Layout layout(uint32_t W, uint32_t H, uint32_t loShift) {
   const uint32_t hN = W * H, G = H / kR;
-  const int twWn = owl::tw_offsets((int)W, 16 / kR).total, twHn = owl::tw_offsets((int)H, 8).total;
+  const int vH = owl::p2_vpt((int)H);
+  const int twWn = owl::tw_offsets((int)W, 16 / kR).total, twHn = owl::tw_offsets((int)H, vH / 2, 0, vH).total;
   Layout L{};
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t at = o; o = up256(o + bytes); return at; };
@@ -106,9 +107,10 @@ __device__ owl::C droot(uint32_t n, uint64_t k) {
 __global__ void k_noalloc_tables(owl::Args a, uint32_t twWn, uint32_t twHn) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const uint32_t W = a.W, H = a.H, N = a.N;
-  auto stage = [&](owl::C* tab, uint32_t n, uint32_t rl, uint32_t i) {
-    const owl::TwOffsets o = owl::tw_offsets((int)n, (int)rl);
-    const uint32_t r1 = owl::plan_r1(n, rl), m1 = owl::plan_m1(n, rl), m2 = owl::plan_m2(n, rl);
+  auto stage = [&](owl::C* tab, uint32_t n, uint32_t rl, uint32_t vmax, uint32_t i) {
+    const owl::TwOffsets o = owl::tw_offsets((int)n, (int)rl, 0, (int)vmax);
+    const uint32_t r1 = owl::plan_r1(n, rl, 0, vmax), m1 = owl::plan_m1(n, rl, 0, vmax),
+                   m2 = owl::plan_m2(n, rl, 0, vmax);
     // which stage table does entry i belong to
     int off;
     uint32_t R, NS;
@@ -121,8 +123,9 @@ __global__ void k_noalloc_tables(owl::Args a, uint32_t twWn, uint32_t twHn) {
     const uint32_t e = i - off, r = e / NS, k = e % NS;
     tab[i] = droot(R * NS, (uint64_t)r * k);
   };
-  for (uint32_t i = tid; i < twWn; i += nth) { stage(const_cast<owl::C*>(a.twW), W, 16 / kR, i); }
-  for (uint32_t i = tid; i < twHn; i += nth) { stage(const_cast<owl::C*>(a.twH), H, 8, i); }
+  const uint32_t vH = (uint32_t)owl::p2_vpt((int)H);
+  for (uint32_t i = tid; i < twWn; i += nth) { stage(const_cast<owl::C*>(a.twW), W, 16 / kR, 16, i); }
+  for (uint32_t i = tid; i < twHn; i += nth) { stage(const_cast<owl::C*>(a.twH), H, vH / 2, vH, i); }
   for (uint32_t i = tid; i < H; i += nth) { const_cast<owl::C*>(a.rootH)[i] = droot(H, i); }
   const uint32_t S = 1u << a.loShift;
   for (uint32_t i = tid; i < S; i += nth) { const_cast<owl::C*>(a.twLo)[i] = droot(a.hN, i); }
@@ -296,7 +299,8 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
   a.timeoutNs = 2000000000ull;
   owl::C* F = reinterpret_cast<owl::C*>(base + L.F);
 
-  const int twWn = owl::tw_offsets((int)W, 16 / kR).total, twHn = owl::tw_offsets((int)H, 8).total;
+  const int vH = owl::p2_vpt((int)H);
+  const int twWn = owl::tw_offsets((int)W, 16 / kR).total, twHn = owl::tw_offsets((int)H, vH / 2, 0, vH).total;
   k_noalloc_tables<<<64, 256, 0, s>>>(a, (uint32_t)twWn, (uint32_t)twHn);
   if (n > 0) {
     const int ll = (flags & OWL_SQ_LL) ? owl::FL_LL : 0;

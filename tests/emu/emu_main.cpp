@@ -170,6 +170,7 @@ void pass2(EmuPlan& p, int mode, C* F, const C* Fb, C* Fq) {
     case 512: p2h<512>(p, mode, F, Fb, Fq); break;
     case 640: p2h<640>(p, mode, F, Fb, Fq); break;
     case 1280: p2h<1280>(p, mode, F, Fb, Fq); break;
+    case 2560: p2h<2560>(p, mode, F, Fb, Fq); break;
     case 2048: p2h<2048>(p, mode, F, Fb, Fq); break;
     default: throw std::runtime_error("emu H");
   }

@@ -87,6 +87,7 @@ def splitmix_words(E, seed):
 @pytest.mark.parametrize("E,W,H,n,seed", [
     (1300021, 64, 640, 3, 7),     # 5 * 2^14 words, radix plan 16 * 5 * 8
     (2500009, 64, 1280, 2, 9),    # 5 * 2^15 words, radix plan 16 * 2 * 5 * 8
+    (5600027, 64, 2560, 2, 11),   # 5 * 2^16 words, radix plan 16 * 4 * 5 * 8 (the 20M column FFT)
 ])
 def test_emulated_radix5_random_start(emu, oracle, E, W, H, n, seed):
     roe, got = run(emu, "square", E, W, H, n, 0, seed)

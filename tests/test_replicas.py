@@ -44,3 +44,24 @@ def test_reference_arm_other_ranks_exit_quietly():
 def test_single_rank_summary_without_process_group():
     import bench
     assert bench.replica_summary(None, 80.0, 9.0, steps=4, block=500, world=1) == (80.0, 9.0, 80.0 / 2000)
+
+
+def test_default_line_runs_every_other_configuration(monkeypatch):
+    """The default (8M, one GPU) line carries a short run of each other configuration, each through
+    its own workload's code path with at least 3 warm-up steps."""
+    import argparse
+    import bench
+    calls = []
+
+    def fake(args, rank, world, local):
+        calls.append((args.workload, args.steps, args.warmup))
+        return {"workload": args.workload}
+
+    monkeypatch.setattr(bench, "run_prp_config", fake)
+    monkeypatch.setattr(bench, "run_batch64", fake)
+    args = argparse.Namespace(workload="prp8m", steps=10, warmup=3, block=1000, no_cpu_baseline=False)
+    out = bench.other_configs(args, 0, 1, 0)
+    assert sorted(out) == ["batch64", "prp20m", "prp256k"]
+    assert all(out[w]["workload"] == w for w in out)
+    assert all(s >= 1 and w >= 3 for _, s, w in calls)
+    assert args.workload == "prp8m" and args.steps == 10      # the caller's arguments are left alone
