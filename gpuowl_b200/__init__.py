@@ -22,6 +22,15 @@ LIB_PATH = os.path.join(_HERE, "libowl.so")
 SQ_MUL3 = 1
 SQ_LL = 2
 SQ_NO_ROE = 4
+# column-pass tile variants (include/owl.h OWL_COL_*)
+COL_AUTO, COL_V16, COL_V8, COL_V16_OCC2 = 0, 1, 2, 3
+COL_NAMES = {COL_V16: "v16", COL_V8: "v8", COL_V16_OCC2: "v16occ2"}
+
+
+def column_variant_supported(H, variant):
+    """Whether the column variant is built for columns of H points."""
+    return bool(load().owl_column_variant_supported(int(H), int(variant)))
+
 
 OK = 0
 ERR_TIMEOUT = -4
@@ -47,7 +56,7 @@ class RunOpts(ctypes.Structure):
                 ("H", ctypes.c_uint32), ("save_dir", ctypes.c_char_p), ("inject_fault_k", ctypes.c_uint32),
                 ("verbose", ctypes.c_int), ("res_cap", ctypes.c_uint32), ("res_k", ctypes.POINTER(ctypes.c_uint32)),
                 ("res_res64", ctypes.POINTER(ctypes.c_uint64)), ("res_n", ctypes.POINTER(ctypes.c_uint32)),
-                ("split", ctypes.c_int), ("proof_power", ctypes.c_uint32)]
+                ("split", ctypes.c_int), ("proof_power", ctypes.c_uint32), ("column_variant", ctypes.c_uint32)]
 
 
 class RunResult(ctypes.Structure):
@@ -73,6 +82,9 @@ _SIGS = {
     "owl_plan_shape": ([_P, _U32P, _U32P, _U32P], ctypes.c_int),
     "owl_plan_set_timeout": ([_P, ctypes.c_uint64], ctypes.c_int),
     "owl_plan_set_split": ([_P, ctypes.c_int], ctypes.c_int),
+    "owl_plan_set_column_variant": ([_P, ctypes.c_uint32], ctypes.c_int),
+    "owl_plan_column_variant": ([_P, _U32P], ctypes.c_int),
+    "owl_column_variant_supported": ([ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int),
     "owl_buf_alloc": ([_P, ctypes.POINTER(_P)], ctypes.c_int),
     "owl_buf_free": ([_P, _P], ctypes.c_int),
     "owl_buf_copy": ([_P, _P, _P], ctypes.c_int),
@@ -189,7 +201,7 @@ class Plan:
     balanced int32 digits in natural word order.
     """
 
-    def __init__(self, E, device=0, W=0, H=0, split=False):
+    def __init__(self, E, device=0, W=0, H=0, split=False, column_variant=0):
         self.lib = load()
         self.E = int(E)
         self.device = device
@@ -203,6 +215,8 @@ class Plan:
         self.split = False
         if split:
             self.set_split(True)
+        if column_variant != COL_AUTO:
+            self.set_column_variant(column_variant)
 
     def close(self):
         if getattr(self, "h", None):
@@ -244,6 +258,17 @@ class Plan:
         inverse 32-point stages of every column FFT (H = 2048 only)."""
         _check(self.lib.owl_plan_set_split(self.h, 1 if enable else 0))
         self.split = bool(enable)
+
+    def set_column_variant(self, variant):
+        """Column-pass tile variant: COL_V16, COL_V8, COL_V16_OCC2, or COL_AUTO for the shape's
+        default (include/owl.h)."""
+        _check(self.lib.owl_plan_set_column_variant(self.h, int(variant)))
+
+    @property
+    def column_variant(self):
+        v = ctypes.c_uint32(0)
+        _check(self.lib.owl_plan_column_variant(self.h, ctypes.byref(v)))
+        return v.value
 
     def write_digits(self, buf, digits):
         d = np.ascontiguousarray(digits, dtype=np.int32)
@@ -330,14 +355,14 @@ class Plan:
 # ---- host drivers (include/owl_host.h) ----
 
 def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, W, H, inject_fault_k, verbose,
-         n_savefiles=4, cap=4096, split=False, proof_power=0):
+         n_savefiles=4, cap=4096, split=False, proof_power=0, column_variant=0):
     lib = load()
     ks = (ctypes.c_uint32 * cap)()
     rs = (ctypes.c_uint64 * cap)()
     n = ctypes.c_uint32(0)
     o = RunOpts(block, log_step, check_step, stop_after, n_savefiles, W, H,
                 save_dir.encode() if save_dir else None, inject_fault_k, 1 if verbose else 0, cap,
-                ks, rs, ctypes.pointer(n), 1 if split else 0, int(proof_power))
+                ks, rs, ctypes.pointer(n), 1 if split else 0, int(proof_power), int(column_variant))
     r = RunResult()
     _check(getattr(lib, fn_name)(device, E, ctypes.byref(o), ctypes.byref(r)))
     return {"is_prime": bool(r.is_prime), "finished": bool(r.finished), "k": r.k, "res64": r.res64,
@@ -349,11 +374,11 @@ def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, 
 
 
 def prp_run(E, device=0, block=1000, log_step=20000, check_step=0, stop_after=0, save_dir=None, W=0, H=0,
-            inject_fault_k=0, verbose=False, split=False, proof_power=0):
+            inject_fault_k=0, verbose=False, split=False, proof_power=0, column_variant=0):
     """PRP-3 test (the reference's Gpu::isPrimePRP) through owl_prp_run; with proof_power > 0 the
     proof residues go to save_dir/<E>/proof/ and the verified proof to save_dir/proof/<E>-<p>.proof."""
     return _run("owl_prp_run", E, device, block, log_step, check_step, stop_after, save_dir, W, H,
-                inject_fault_k, verbose, split=split, proof_power=proof_power)
+                inject_fault_k, verbose, split=split, proof_power=proof_power, column_variant=column_variant)
 
 
 class Task(ctypes.Structure):
@@ -433,9 +458,11 @@ def proof_verify(path, device=0):
     return bool(v.value), bool(p.value)
 
 
-def ll_run(E, device=0, log_step=10000, stop_after=0, save_dir=None, W=0, H=0, verbose=False, split=False):
+def ll_run(E, device=0, log_step=10000, stop_after=0, save_dir=None, W=0, H=0, verbose=False, split=False,
+           column_variant=0):
     """Lucas-Lehmer test (the reference's Gpu::isPrimeLL) through owl_ll_run."""
-    return _run("owl_ll_run", E, device, 1000, log_step, 0, stop_after, save_dir, W, H, 0, verbose, split=split)
+    return _run("owl_ll_run", E, device, 1000, log_step, 0, stop_after, save_dir, W, H, 0, verbose, split=split,
+                column_variant=column_variant)
 
 
 def prp_save(save_dir, E, k, block, res64, check, n_errors=0, elapsed=0.0):

@@ -115,6 +115,11 @@ struct owl_plan {
   };
   std::vector<GraphEntry> graphs;
   uint64_t useClock = 0;
+  // column variant (owl::COL_V16 / COL_V8 / COL_V16_OCC2) and the device copies of its stage
+  // tables (COL_V16_OCC2 shares COL_V16's)
+  int colVariant = owl::COL_V16;
+  const C* twHv16 = nullptr;
+  const C* twHv8 = nullptr;
   // split-precision column pass (H = 2048 only): DFT digit planes and its stage tables
   bool split = false;
   const unsigned char* tcB = nullptr;
@@ -145,15 +150,21 @@ template <int W, int M> void setp1attr() {
        "cudaFuncSetAttribute(pass1 group without round-off)");
   }
 }
-template <int H, int M> void setp2attr() {
-  constexpr int V = owl::p2_vpt(H);
+template <int H, int M, int CV> void setp2attr_v() {
+  constexpr int V = owl::col_vpt(CV), MB = owl::col_minb(CV);
   size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
-  ck(cudaFuncSetAttribute(owl::k_pass2<H, kR, M, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+  ck(cudaFuncSetAttribute(owl::k_pass2<H, kR, M, V, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
      "cudaFuncSetAttribute(pass2)");
   if (M == owl::P2_SQUARE) {
-    ck(cudaFuncSetAttribute(owl::k_pass2_group<H, kR, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
+    ck(cudaFuncSetAttribute(owl::k_pass2_group<H, kR, V, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
        "cudaFuncSetAttribute(pass2 group)");
   }
+}
+// every column variant built for H
+template <int H, int M> void setp2attr() {
+  setp2attr_v<H, M, owl::COL_V16>();
+  if constexpr (owl::col_variant_ok(H, owl::COL_V8)) { setp2attr_v<H, M, owl::COL_V8>(); }
+  if constexpr (owl::col_variant_ok(H, owl::COL_V16_OCC2)) { setp2attr_v<H, M, owl::COL_V16_OCC2>(); }
 }
 
 template <int M> void setp2tcattr() {
@@ -211,15 +222,27 @@ template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int 
   launch_pass(p, pdl, k, grid, T, sm, p->args, F, words, roeSlot, flags, ts);
 }
 
-template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
-  constexpr int V = owl::p2_vpt(H);
+template <int H, int CV> void p2launch_v(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
+  constexpr int V = owl::col_vpt(CV), MB = owl::col_minb(CV);
   constexpr int T = 2 * H / V;
   size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
   dim3 grid(p->W / 2);
-  auto k = (mode == owl::P2_SQUARE) ? owl::k_pass2<H, kR, owl::P2_SQUARE, V>
-           : (mode == owl::P2_FWD)  ? owl::k_pass2<H, kR, owl::P2_FWD, V>
-                                    : owl::k_pass2<H, kR, owl::P2_MUL, V>;
+  auto k = (mode == owl::P2_SQUARE) ? owl::k_pass2<H, kR, owl::P2_SQUARE, V, MB>
+           : (mode == owl::P2_FWD)  ? owl::k_pass2<H, kR, owl::P2_FWD, V, MB>
+                                    : owl::k_pass2<H, kR, owl::P2_MUL, V, MB>;
   launch_pass(p, pdl, k, grid, T, sm, p->args, F, Fb, Fq, ts);
+}
+// the plan's column variant (checked against H when it was set)
+template <int H> void p2launch(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
+  if constexpr (owl::col_variant_ok(H, owl::COL_V8)) {
+    if (p->colVariant == owl::COL_V8) { return p2launch_v<H, owl::COL_V8>(p, mode, F, Fb, Fq, ts, pdl); }
+  }
+  if constexpr (owl::col_variant_ok(H, owl::COL_V16_OCC2)) {
+    if (p->colVariant == owl::COL_V16_OCC2) {
+      return p2launch_v<H, owl::COL_V16_OCC2>(p, mode, F, Fb, Fq, ts, pdl);
+    }
+  }
+  p2launch_v<H, owl::COL_V16>(p, mode, F, Fb, Fq, ts, pdl);
 }
 
 #define OWL_FOR_SIZES(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
@@ -356,18 +379,28 @@ template <int W> void p1group(cudaStream_t st, int mode, bool roe, const owl::Gr
                                    : owl::k_pass1_group<W, kR, owl::P1_OUT>;
   launch_on(st, mode != owl::P1_IN, k, grid, T, sm, ga, roeSlot, flags);
 }
-template <int H> void p2group(cudaStream_t st, const owl::GroupArgs& ga, uint32_t cnt, uint32_t W) {
-  constexpr int V = owl::p2_vpt(H);
+template <int H, int CV> void p2group_v(cudaStream_t st, const owl::GroupArgs& ga, uint32_t cnt, uint32_t W) {
+  constexpr int V = owl::col_vpt(CV), MB = owl::col_minb(CV);
   const size_t sm = 2 * (size_t)owl::p2_col_stride<H, V>() * sizeof(C);
-  launch_on(st, true, owl::k_pass2_group<H, kR, V>, dim3(W / 2, cnt), 2 * H / V, sm, ga);
+  launch_on(st, true, owl::k_pass2_group<H, kR, V, MB>, dim3(W / 2, cnt), 2 * H / V, sm, ga);
+}
+template <int H> void p2group(cudaStream_t st, const owl::GroupArgs& ga, uint32_t cnt, uint32_t W, int cv) {
+  if constexpr (owl::col_variant_ok(H, owl::COL_V8)) {
+    if (cv == owl::COL_V8) { return p2group_v<H, owl::COL_V8>(st, ga, cnt, W); }
+  }
+  if constexpr (owl::col_variant_ok(H, owl::COL_V16_OCC2)) {
+    if (cv == owl::COL_V16_OCC2) { return p2group_v<H, owl::COL_V16_OCC2>(st, ga, cnt, W); }
+  }
+  p2group_v<H, owl::COL_V16>(st, ga, cnt, W);
 }
 
 // n squarings of each plan's buffer (in place) as grouped launches on `st`: plans of one plain
-// (not split-precision) shape, at most kGroupMax
+// (not split-precision) shape and column variant, at most kGroupMax
 void enqueue_square_group(cudaStream_t st, const std::vector<owl_plan*>& plans, const std::vector<int32_t*>& bufs,
                           uint32_t n, uint32_t flags) {
   const uint32_t cnt = (uint32_t)plans.size();
   const uint32_t W = plans[0]->W, H = plans[0]->H;
+  const int cv = plans[0]->colVariant;
   owl::GroupArgs ga{};
   for (uint32_t i = 0; i < cnt; ++i) {
     ga.a[i] = plans[i]->args;
@@ -393,7 +426,7 @@ void enqueue_square_group(cudaStream_t st, const std::vector<owl_plan*>& plans, 
     switch (H) {
 #define CASE_H(x)                            \
   case x:                                    \
-    p2group<x>(st, ga, cnt, W);              \
+    p2group<x>(st, ga, cnt, W, cv);          \
     break;
       OWL_FOR_H_SIZES(CASE_H)
 #undef CASE_H
@@ -483,6 +516,16 @@ void sync_and_check(owl_plan* p) {
   }
 }
 
+static_assert(OWL_COL_AUTO == owl::COL_AUTO && OWL_COL_V16 == owl::COL_V16 && OWL_COL_V8 == owl::COL_V8 &&
+                  OWL_COL_V16_OCC2 == owl::COL_V16_OCC2,
+              "column variant numbers of owl.h and the kernels");
+
+// the column variant's kernels and stage tables (the variant checked against H by the caller)
+void apply_col_variant(owl_plan* p, int cv) {
+  p->colVariant = cv;
+  p->args.twH = (cv == owl::COL_V8) ? p->twHv8 : p->twHv16;
+}
+
 template <typename T> T* carve(char*& cur, size_t count) {
   size_t off = (reinterpret_cast<uintptr_t>(cur) + 255) & ~uintptr_t(255);
   T* r = reinterpret_cast<T*>(off);
@@ -528,8 +571,11 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   const bool tcShape = (H == (uint32_t)owl::kTcH);
   const std::vector<owl::HostC> twHtc = tcShape ? owl::stage_tables(H, 8, owl::kTcR1) : std::vector<owl::HostC>();
   const std::vector<uint8_t> tcB = tcShape ? owl::tc_dft_digits() : std::vector<uint8_t>();
-  size_t nC = t.twW.size() + t.twH.size() + t.rootH.size() + t.twLo.size() + t.twHi.size() + twHtc.size();
-  size_t bytes = 256 * 16 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
+  const std::vector<owl::HostC> twH8 =
+      owl::col_variant_ok((int)H, owl::COL_V8) ? owl::col_stage_tables(H, owl::COL_V8) : std::vector<owl::HostC>();
+  size_t nC = t.twW.size() + t.twH.size() + twH8.size() + t.rootH.size() + t.twLo.size() + t.twHi.size() +
+              twHtc.size();
+  size_t bytes = 256 * 18 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
                  (t.x1.size() + t.x2.size() + t.p1masks.size()) * sizeof(uint32_t) + tcB.size();
   ck(cudaMalloc(&p->tableMem, bytes), "cudaMalloc(tables)");
   std::vector<char> host(bytes, 0);
@@ -542,7 +588,8 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   };
   char* dbase = static_cast<char*>(p->tableMem);
   p->args.twW = reinterpret_cast<const C*>(dbase + put(t.twW.data(), t.twW.size() * sizeof(C)));
-  p->args.twH = reinterpret_cast<const C*>(dbase + put(t.twH.data(), t.twH.size() * sizeof(C)));
+  p->twHv16 = reinterpret_cast<const C*>(dbase + put(t.twH.data(), t.twH.size() * sizeof(C)));
+  if (!twH8.empty()) { p->twHv8 = reinterpret_cast<const C*>(dbase + put(twH8.data(), twH8.size() * sizeof(C))); }
   p->args.rootH = reinterpret_cast<const C*>(dbase + put(t.rootH.data(), t.rootH.size() * sizeof(C)));
   p->args.twLo = reinterpret_cast<const C*>(dbase + put(t.twLo.data(), t.twLo.size() * sizeof(C)));
   p->args.twHi = reinterpret_cast<const C*>(dbase + put(t.twHi.data(), t.twHi.size() * sizeof(C)));
@@ -600,6 +647,7 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
   p->args.iscaleLo = std::ldexp(1.0, -(int)(E / N));
   p->args.loShift = t.loShift;
   p->args.timeoutNs = 2000000000ull;
+  apply_col_variant(p.get(), owl::default_col_variant(W, H));
   *out = p.release();
 }
 
@@ -792,6 +840,33 @@ int owl_plan_set_split(owl_plan* plan, int enable) {
     plan->graphs.clear();
     plan->split = enable != 0;
   });
+}
+
+int owl_plan_set_column_variant(owl_plan* plan, uint32_t variant) {
+  return guarded([&] {
+    check_plan(plan);
+    const int cv = variant == OWL_COL_AUTO ? owl::default_col_variant(plan->W, plan->H) : (int)variant;
+    if (variant > OWL_COL_V16_OCC2 || !owl::col_variant_ok((int)plan->H, cv)) {
+      fail(OWL_ERR_ARG, "column variant not built for this height");
+    }
+    DeviceGuard dg(plan->device);
+    ck(cudaStreamSynchronize(plan->stream), "cudaStreamSynchronize");
+    for (auto& g : plan->graphs) { cudaGraphExecDestroy(g.exec); }
+    plan->graphs.clear();
+    apply_col_variant(plan, cv);
+  });
+}
+
+int owl_plan_column_variant(const owl_plan* plan, uint32_t* variant) {
+  return guarded([&] {
+    check_plan(plan);
+    if (!variant) { fail(OWL_ERR_ARG, "null out"); }
+    *variant = (uint32_t)plan->colVariant;
+  });
+}
+
+int owl_column_variant_supported(uint32_t H, uint32_t variant) {
+  return variant >= OWL_COL_V16 && variant <= OWL_COL_V16_OCC2 && owl::col_variant_ok((int)H, (int)variant) ? 1 : 0;
 }
 
 int owl_buf_alloc(owl_plan* plan, int32_t** buf) {
@@ -1127,7 +1202,8 @@ cudaGraphExec_t batch_graph(owl_batch* b, int32_t* const* bufs, uint32_t n, uint
     std::vector<std::pair<uint64_t, size_t>> order;
     for (size_t i = 0; i < b->plans.size(); ++i) {
       const owl_plan* p = b->plans[i];
-      const uint64_t key = p->split ? (1ull << 63) | i : ((uint64_t)p->W << 32) | p->H;
+      const uint64_t key =
+          p->split ? (1ull << 63) | i : ((uint64_t)p->W << 32) | ((uint64_t)p->H << 4) | (uint64_t)p->colVariant;
       order.push_back({key, i});
     }
     std::stable_sort(order.begin(), order.end());

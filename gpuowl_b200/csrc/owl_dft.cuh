@@ -314,14 +314,23 @@ constexpr int plan_m2(int n, int rl, int r1f = 0, int vmax = 16) {
   return plan_rest2(n, rl, r1f, vmax) / plan_m1(n, rl, r1f, vmax);
 }
 
-// values per thread of the column pass for column length H: 8 (twice the threads at half the
-// registers) for power-of-two H <= 2048 when built with OWL_P2_VPT=8, else 16
-#ifndef OWL_P2_VPT
-#define OWL_P2_VPT 16
-#endif
-__host__ __device__ constexpr int p2_vpt(int H) {
-  return (OWL_P2_VPT == 8 && (H & (H - 1)) == 0 && H <= 2048) ? 8 : 16;
+// Column-pass tile variants, chosen per plan (owl_plan_set_column_variant; gpuowl_b200.tune times
+// them per shape): the values a thread holds (which fixes the radix plan and the threads of a CTA)
+// and the CTAs per SM that the launch bounds ask for.
+//   COL_V16       16 values a thread, H/8 threads a CTA: every H
+//   COL_V8         8 values a thread, H/4 threads (twice the threads at half the registers; the radix
+//                  plan 8 x ... x 4): H a power of two up to 2048, 640 and 1280
+//   COL_V16_OCC2  16 values a thread at two CTAs per SM (102 registers, a few spilled): H = 2560,
+//                  whose default runs one 320-thread CTA of 168 registers per SM
+// COL_AUTO (0) stands for the shape's default (owl_tables.hpp: default_col_variant).
+enum : int { COL_AUTO = 0, COL_V16 = 1, COL_V8 = 2, COL_V16_OCC2 = 3 };
+__host__ __device__ constexpr bool col_variant_ok(int H, int v) {
+  return v == COL_V16 || (v == COL_V8 && ((((H & (H - 1)) == 0) && H <= 2048) || H == 640 || H == 1280)) ||
+         (v == COL_V16_OCC2 && H == 2560);
 }
+__host__ __device__ constexpr int col_vpt(int v) { return v == COL_V8 ? 8 : 16; }
+// the CTAs per SM of the column pass's launch bounds (0: the kernel's own rule)
+__host__ __device__ constexpr int col_minb(int v) { return v == COL_V16_OCC2 ? 2 : 0; }
 
 // CTAs per SM that the pass kernels' launch bounds ask for: enough for 16 resident warps at most
 // 128 registers a thread (T threads a CTA; at most 32 CTAs an SM). Without the hint the kernels of

@@ -42,7 +42,7 @@ struct Args {
   double scaleLo;      // 2^bitsLo
   double iscaleLo;     // 2^-bitsLo
   const C* twW;    // stage tables of the width FFT (tw_offsets(W, 16/R) layout)
-  const C* twH;    // stage tables of the height FFT (tw_offsets(H, p2_vpt(H) / 2, 0, p2_vpt(H)) layout)
+  const C* twH;    // stage tables of the height FFT (tw_offsets(H, V / 2, 0, V) layout, V = col_vpt(variant))
   const C* rootH;  // w_H^i, i < H
   const C* twLo;   // w_hN^i, i < 2^loShift
   const C* twHi;   // w_hN^(i << loShift)
@@ -202,10 +202,10 @@ __device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
 
 // VPT: values per thread (16, or 8 for twice the threads at half the registers); the
 // cross-column last stage has radix RL = VPT/2 (A and B butterflies in one thread).
-// Occupancy hint: 2 CTAs per SM for the 256-thread (and 512-thread VPT 8) columns; 3 for the
-// 160-thread H = 1280 columns, which otherwise take 243 registers and run one 5-warp CTA per SM
+// Occupancy hint (MINB = 0): 2 CTAs per SM for the 256-thread (and 512-thread VPT 8) columns; 3 for
+// the 160-thread H = 1280 columns, which otherwise take 243 registers and run one 5-warp CTA per SM
 // (5M: 45.5 -> 32.6 us per column pass with a few spilled registers). The 320-thread H = 2560
-// columns stay at one CTA: two would cap them at 102 registers.
+// columns take one CTA, or two with MINB = 2 (the COL_V16_OCC2 variant: 102 registers).
 
 // ---------------------------------------------------------------------------
 // The pass kernels: one plan (k_pass1, k_pass2), or the same pass of up to kGroupMax plans of one
@@ -222,9 +222,11 @@ __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
 #include "owl_pass1_body.inc"
 }
 
-template <int H, int R, int MODE, int VPT = 16>
+template <int H, int R, int MODE, int VPT = 16, int MINB = 0>
 __global__ void __launch_bounds__(2 * H / VPT,
-                                  ((2 * H / VPT == 256) || (VPT == 8 && 2 * H / VPT == 512)) ? 2 : (H == 1280 ? 3 : 1))
+                                  MINB ? MINB
+                                       : (((2 * H / VPT == 256) || (VPT == 8 && 2 * H / VPT == 512)) ? 2
+                                                                                                     : (H == 1280 ? 3 : 1)))
     k_pass2(Args a, C* __restrict__ F, const C* __restrict__ Fb, C* __restrict__ Fq, int tslot) {
   const uint32_t blk = blockIdx.x;
 #include "owl_pass2_body.inc"
@@ -254,9 +256,12 @@ __global__ void __launch_bounds__(R * W / 16, occ_blocks(R * W / 16))
 #include "owl_pass1_body.inc"
 }
 
-template <int H, int R, int VPT = 16>
-__global__ void __launch_bounds__(2 * H / VPT, (VPT == 8 && 2 * H / VPT == 512) ? 2
-                                                : (H == 1280 ? 3 : (H == 2560 ? 1 : occ_blocks(2 * H / VPT))))
+template <int H, int R, int VPT = 16, int MINB = 0>
+__global__ void __launch_bounds__(2 * H / VPT,
+                                  MINB ? MINB
+                                       : ((VPT == 8 && 2 * H / VPT == 512)
+                                              ? 2
+                                              : (H == 1280 ? 3 : (H == 2560 ? 1 : occ_blocks(2 * H / VPT)))))
     k_pass2_group(const __grid_constant__ GroupArgs ga) {
   constexpr int MODE = P2_SQUARE;
   const Args& a = ga.a[blockIdx.y];

@@ -69,7 +69,7 @@ struct Layout {
 };
 Layout layout(uint32_t W, uint32_t H, uint32_t loShift) {
   const uint32_t hN = W * H, G = H / kR;
-  const int vH = owl::p2_vpt((int)H);
+  const int vH = owl::col_vpt(owl::COL_V16);  // the default column variant's kernels
   const int twWn = owl::tw_offsets((int)W, 16 / kR).total, twHn = owl::tw_offsets((int)H, vH / 2, 0, vH).total;
   Layout L{};
   size_t o = 0;
@@ -123,7 +123,7 @@ __global__ void k_noalloc_tables(owl::Args a, uint32_t twWn, uint32_t twHn) {
     const uint32_t e = i - off, r = e / NS, k = e % NS;
     tab[i] = droot(R * NS, (uint64_t)r * k);
   };
-  const uint32_t vH = (uint32_t)owl::p2_vpt((int)H);
+  const uint32_t vH = (uint32_t)owl::col_vpt(owl::COL_V16);
   for (uint32_t i = tid; i < twWn; i += nth) { stage(const_cast<owl::C*>(a.twW), W, 16 / kR, 16, i); }
   for (uint32_t i = tid; i < twHn; i += nth) { stage(const_cast<owl::C*>(a.twH), H, vH / 2, vH, i); }
   for (uint32_t i = tid; i < H; i += nth) { const_cast<owl::C*>(a.rootH)[i] = droot(H, i); }
@@ -299,7 +299,7 @@ extern "C" int owl_square_noalloc(int device, uint32_t E, uint32_t W, uint32_t H
   a.timeoutNs = 2000000000ull;
   owl::C* F = reinterpret_cast<owl::C*>(base + L.F);
 
-  const int vH = owl::p2_vpt((int)H);
+  const int vH = owl::col_vpt(owl::COL_V16);  // the default column variant's kernels
   const int twWn = owl::tw_offsets((int)W, 16 / kR).total, twHn = owl::tw_offsets((int)H, vH / 2, 0, vH).total;
   k_noalloc_tables<<<64, 256, 0, s>>>(a, (uint32_t)twWn, (uint32_t)twHn);
   if (n > 0) {

@@ -77,6 +77,21 @@ inline std::vector<HostC> stage_tables(uint32_t n, uint32_t rl, uint32_t r1f = 0
   return t;
 }
 
+// the column FFT's stage tables for a column variant (its values a thread V: tw_offsets(H, V/2, 0, V))
+inline std::vector<HostC> col_stage_tables(uint32_t H, int variant) {
+  const uint32_t v = (uint32_t)col_vpt(variant);
+  return stage_tables(H, v / 2, 0, v);
+}
+
+// The column variant a plan of shape W x H starts with: the fastest of the variants built for H as
+// measured on B200 by gpuowl_b200.tune --variants (the reference's built-in tune defaults play the
+// same part, src/TuneEntry.cpp); owl_plan_set_column_variant overrides it.
+inline int default_col_variant(uint32_t W, uint32_t H) {
+  (void)W;
+  (void)H;
+  return COL_V16;
+}
+
 struct Tables {
   uint32_t E = 0, N = 0, W = 0, H = 0, hN = 0, loShift = 0;
   std::vector<HostC> twW, twH, rootH, twLo, twHi;
@@ -164,10 +179,7 @@ inline Tables make_tables(uint32_t E, uint32_t W, uint32_t H) {
   const uint32_t N = t.N;
   t.loShift = (log2u(t.hN) + 1) / 2;
   t.twW = stage_tables(W, 16 / kLinesPerBlock);
-  {
-    const uint32_t v = (uint32_t)p2_vpt((int)H);  // the column pass's values per thread
-    t.twH = stage_tables(H, v / 2, 0, v);
-  }
+  t.twH = col_stage_tables(H, COL_V16);
   t.rootH.resize(H);
   for (uint32_t i = 0; i < H; ++i) { t.rootH[i] = root(H, i); }
   uint32_t S = 1u << t.loShift;

@@ -327,9 +327,10 @@ class SaveDir {
 // ---- the engine, as the reference's Gpu sees it ----
 class HostGpu {
  public:
-  HostGpu(int device, uint32_t E, uint32_t W, uint32_t H, int split = 0) : E_(E) {
+  HostGpu(int device, uint32_t E, uint32_t W, uint32_t H, int split = 0, uint32_t colVariant = 0) : E_(E) {
     ck(owl_plan_create(device, E, W, H, &plan_));
     if (split) { ck(owl_plan_set_split(plan_, 1)); }
+    if (colVariant) { ck(owl_plan_set_column_variant(plan_, colVariant)); }
     ck(owl_buf_alloc(plan_, &data));
     ck(owl_buf_alloc(plan_, &check));
     ck(owl_buf_alloc(plan_, &aux));
@@ -833,7 +834,7 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
   const uint32_t B0 = o.block_size ? o.block_size : 1000;
   const uint32_t logStep = o.log_step ? o.log_step : 20000;
   if (B0 % 100 != 0 || 10000 % B0 != 0 || logStep % B0 != 0) { fail(OWL_ERR_ARG, "block size / log step"); }
-  HostGpu gpu(device, E, o.W, o.H, o.split);
+  HostGpu gpu(device, E, o.W, o.H, o.split, o.column_variant);
   SaveDir saver(o.save_dir, E, true, o.n_savefiles);
   Log log{o};
   if (o.res_n) { *o.res_n = 0; }
@@ -974,7 +975,7 @@ void prp(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
 // Gpu::isPrimeLL (src/Gpu.cpp:1586-1663)
 void ll(int device, uint32_t E, const owl_run_opts& o, owl_run_result& res) {
   const uint32_t logStep = o.log_step ? o.log_step : 10000;
-  HostGpu gpu(device, E, o.W, o.H, o.split);
+  HostGpu gpu(device, E, o.W, o.H, o.split, o.column_variant);
   SaveDir saver(o.save_dir, E, false, o.n_savefiles);
   Log log{o};
   if (o.res_n) { *o.res_n = 0; }

@@ -6,12 +6,17 @@ each FFT with Gpu::timePRP and writes tune.txt).
 
 For every FFT size N = 2^lg, and N = 5 * 2^(lg-3) with --five, it times each W x H split the library
 supports (W a power of two in [64, 4096]; H a power of two in [64, 4096] with H/W in {1/2, 1, 2, 4},
-or H in {640, 1280, 2560}) with owl_profile_square (device time of the two passes per
-squaring, at an exponent of 18 bits per word), keeps the fastest split, and records its max
-round-off. Output:
+or H in {640, 1280, 2560}) and, for each split, every column-pass variant built for its H (the radix
+plan and tile of the column FFT: 16 or 8 values a thread, one or two CTAs per SM; include/owl.h
+OWL_COL_*), by the time per squaring of a graph-launched block (at an exponent of 18 bits per word), keeps the
+fastest, and records its max round-off. Output:
   - tune.txt in the reference's format, "%6.1f %14s # %u" = microseconds per iteration, shape,
-    largest exponent (src/TuneEntry.cpp:94-105), rows in increasing cost and exponent;
-  - tune.json, {"N": [W, H, us_per_iter, max_roe]}, read by fft_choose(..., tune=path).
+    largest exponent (src/TuneEntry.cpp:94-105), rows in increasing cost and exponent, followed by
+    the column variant's name;
+  - tune.json, {"N": [W, H, us_per_iter, max_roe, max_bpw or null, column_variant]}, read by
+    fft_choose(..., tune=path) and tuned_variant(N, path).
+
+    python -m gpuowl_b200.tune --shapes 4096x2560 --variants   # per-pass times of every variant
 """
 import argparse
 import json
@@ -58,7 +63,13 @@ def next_odd_exponent(x):
     return x
 
 
-def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True, five=False):
+def variants_for(H):
+    """The column-pass variants built for columns of H points (OWL_COL_V16 first)."""
+    import gpuowl_b200 as owl
+    return [v for v in (owl.COL_V16, owl.COL_V8, owl.COL_V16_OCC2) if owl.column_variant_supported(H, v)]
+
+
+def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True, five=False, variants=True):
     import numpy as np
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
@@ -68,31 +79,65 @@ def tune(min_lg, max_lg, iters, max_bpw=18.0, device=0, verbose=True, five=False
         E = next_odd_exponent(N * max_bpw * 0.98)
         best = None
         for (W, H) in candidates(N):
-            with owl.Plan(E, device=device, W=W, H=H) as p:
-                b = p.alloc()
-                rng = np.random.default_rng(N)
-                w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
-                if E % 32:
-                    w[-1] &= (1 << (E % 32)) - 1
-                p.writeIn(b, w)
-                p.profile_square(b, 20)  # warm
-                p.readROE()
-                prof = p.profile_square(b, iters)
-                us = 1e3 * (prof["pass2"][0] + prof["pass1"][0] + prof["edge"][0]) / iters
-                roe = float(p.readROE().max())
-            if verbose:
-                print("N=%-9d %-14s %8.2f us/iter  max ROE %.4f" % (N, spec(W, H), us, roe), flush=True)
-            if best is None or us < best[2]:
-                best = (W, H, us, roe)
+            for cv in (variants_for(H) if variants else [owl.COL_AUTO]):
+                with owl.Plan(E, device=device, W=W, H=H, column_variant=cv) as p:
+                    b = p.alloc()
+                    rng = np.random.default_rng(N)
+                    w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
+                    if E % 32:
+                        w[-1] &= (1 << (E % 32)) - 1
+                    p.writeIn(b, w)
+                    p.profile_square(b, 20)  # warm
+                    p.readROE()
+                    p.profile_square(b, iters)
+                    roe = float(p.readROE().max())
+                    us = block_us(p, b, iters)
+                    cv = p.column_variant
+                if verbose:
+                    print("N=%-9d %-14s %-8s %8.2f us/iter  max ROE %.4f"
+                          % (N, spec(W, H), owl.COL_NAMES[cv], us, roe), flush=True)
+                if best is None or us < best[2]:
+                    best = (W, H, us, roe, None, cv)
         if best:
             rows[N] = best
     return rows
 
 
-def profile_shapes(shapes, iters, bpw=16.0, device=0, split=False):
-    """Per-kernel device time of `iters` squarings on each W x H shape (the -time profile per shape):
-    E is the first odd number above N * bpw, the residue random; one untimed block first. With
-    `split` the column pass runs in the split-precision form (H = 2048 only)."""
+def block_us(p, b, iters, reps=2):
+    """Microseconds per squaring of a graph-launched block of `iters` squarings, wall clock from
+    launch to completion (the reference's timePRP measures the same way), best of `reps` blocks.
+    The per-pass stamps of profile_square overlap where a pass starts as a programmatic dependent
+    of the one before, so their sum is not the iteration time."""
+    import time
+    p.squareLoop(b, b, iters)  # captures the block's graph
+    p.sync()
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        p.squareLoop(b, b, iters)
+        p.sync()
+        dt = 1e6 * (time.perf_counter() - t0) / iters
+        best = dt if best is None else min(best, dt)
+    return best
+
+
+def tuned_variant(N, tune_json):
+    """The column variant tune.json holds for FFT size N (OWL_COL_AUTO when it holds none)."""
+    import gpuowl_b200 as owl
+    if not tune_json or not os.path.exists(tune_json):
+        return owl.COL_AUTO
+    with open(tune_json) as f:
+        v = json.load(f).get(str(int(N)))
+    return int(v[5]) if v and len(v) >= 6 and v[5] else owl.COL_AUTO
+
+
+def profile_shapes(shapes, iters, bpw=16.0, device=0, split=False, variants=False):
+    """Per-kernel device time of `iters` squarings on each W x H shape (the -time profile per shape),
+    and the time per squaring of a whole block (block_us): E is the first odd number above N * bpw,
+    the residue random; one untimed block first. With
+    `split` the column pass runs in the split-precision form (H = 2048 only); with `variants` every
+    column variant built for H is timed, else the shape's default. The res64 after the timed block
+    is returned with each row (the same for every variant of a shape)."""
     import numpy as np
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
@@ -101,23 +146,26 @@ def profile_shapes(shapes, iters, bpw=16.0, device=0, split=False):
     for (W, H) in shapes:
         N = 2 * W * H
         E = next_odd_exponent(N * bpw)
-        with owl.Plan(E, device=device, W=W, H=H, split=split) as p:
-            b = p.alloc()
-            rng = np.random.default_rng(N)
-            w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
-            if E % 32:
-                w[-1] &= (1 << (E % 32)) - 1
-            p.writeIn(b, w)
-            p.profile_square(b, iters)
-            p.readROE()
-            prof = p.profile_square(b, iters)
-            roe = float(p.readROE().max())
-        us2 = 1e3 * prof["pass2"][0] / prof["pass2"][1]
-        us1 = 1e3 * prof["pass1"][0] / prof["pass1"][1]
-        total = 1e3 * (prof["pass2"][0] + prof["pass1"][0] + prof["edge"][0]) / iters
-        rows.append((N, W, H, total, us2, us1, roe))
-        print("N=%-9d %-14s %8.2f us/iter  column pass %7.2f us  line pass %7.2f us  max ROE %.4f"
-              % (N, spec(W, H), total, us2, us1, roe), flush=True)
+        for cv in (variants_for(H) if variants else [owl.COL_AUTO]):
+            with owl.Plan(E, device=device, W=W, H=H, split=split, column_variant=cv) as p:
+                b = p.alloc()
+                rng = np.random.default_rng(N)
+                w = rng.integers(0, 2 ** 32, size=p.nwords, dtype=np.uint64).astype(np.uint32)
+                if E % 32:
+                    w[-1] &= (1 << (E % 32)) - 1
+                p.writeIn(b, w)
+                p.profile_square(b, iters)
+                p.readROE()
+                prof = p.profile_square(b, iters)
+                roe = float(p.readROE().max())
+                res = p.bufResidue(b)
+                total = block_us(p, b, iters)
+                cv = p.column_variant
+            us2 = 1e3 * prof["pass2"][0] / prof["pass2"][1]
+            us1 = 1e3 * prof["pass1"][0] / prof["pass1"][1]
+            rows.append((N, W, H, total, us2, us1, roe, cv, res))
+            print("N=%-9d %-14s %-8s %8.2f us/iter  column pass %7.2f us  line pass %7.2f us  max ROE %.4f  "
+                  "res64 %016x" % (N, spec(W, H), owl.COL_NAMES[cv], total, us2, us1, roe, res), flush=True)
     return rows
 
 
@@ -340,12 +388,15 @@ def write_bpw(table, limit, iters, out_txt):
 
 
 def write(rows, max_bpw, out_txt, out_json):
+    import gpuowl_b200 as owl
     lines, prev_cost = [], 0.0
     for N in sorted(rows):
-        W, H, us, roe = rows[N]
+        W, H, us, roe = rows[N][:4]
+        cv = rows[N][5] if len(rows[N]) >= 6 else None
         cost = max(us, prev_cost)
         prev_cost = cost
-        lines.append("%6.1f %14s # %u" % (cost, spec(W, H), int(N * max_bpw)))
+        lines.append("%6.1f %14s # %u" % (cost, spec(W, H), int(N * max_bpw)) +
+                     (" " + owl.COL_NAMES[cv] if cv in owl.COL_NAMES else ""))
     with open(out_txt, "w") as f:
         f.write("\n".join(lines) + "\n")
     with open(out_json, "w") as f:
@@ -368,10 +419,13 @@ def main():
                     help="with --bpw-scan: round-off Z = 28 (the reference's) or max round-off < --roe-limit")
     ap.add_argument("--shapes", metavar="WxH,...", help="per-pass times of these shapes (at 16 bits/word)")
     ap.add_argument("--split", action="store_true", help="with --shapes: the split-precision column pass")
+    ap.add_argument("--variants", action="store_true",
+                    help="with --shapes: time every column variant built for the shape's H")
+    ap.add_argument("--no-variants", action="store_true", help="sweep: the shapes' default column variants only")
     a = ap.parse_args()
     if a.shapes:
         profile_shapes([tuple(int(v) for v in s.split("x")) for s in a.shapes.split(",")], a.iters,
-                       split=a.split)
+                       split=a.split, variants=a.variants)
         return
     if a.bpw_scan:
         with open(a.bpw_scan) as f:
@@ -386,12 +440,12 @@ def main():
             write_bpw(table, a.roe_limit, a.iters, a.out)
         for N, (W, H, best, _) in table.items():
             if best and str(N) in t:
-                t[str(N)] = list(t[str(N)][:4]) + [best]
+                t[str(N)] = list(t[str(N)][:4]) + [best] + list(t[str(N)][5:])
         with open(a.json, "w") as f:
             json.dump(t, f, indent=1)
         print(open(a.out).read())
         return
-    rows = tune(a.min_lg, a.max_lg, a.iters, a.bpw, five=a.five)
+    rows = tune(a.min_lg, a.max_lg, a.iters, a.bpw, five=a.five, variants=not a.no_variants)
     write(rows, a.bpw, a.out, a.json)
     print(open(a.out).read())
 

@@ -85,6 +85,27 @@ int owl_plan_set_timeout(owl_plan* plan, uint64_t ns);
    it first ran a block of that size, so set the form before building batches. */
 int owl_plan_set_split(owl_plan* plan, int enable);
 
+/* Column-pass tile variant -- the reference's tune.txt carries, besides the FFT shape, the build
+   options measured fastest for it (src/tune.cpp:106-186, src/TuneEntry.cpp:94-105); here the choice
+   is between kernels built for the same shape with another radix plan and tile:
+     OWL_COL_V16       16 values a thread, H/8 threads a CTA (every H)
+     OWL_COL_V8         8 values a thread, H/4 threads a CTA, radix plan 8 x ... x 4
+                        (H a power of two up to 2048, 640 or 1280)
+     OWL_COL_V16_OCC2  16 values a thread at two CTAs per SM instead of one (H = 2560)
+   OWL_COL_AUTO selects the shape's default (measured on B200, gpuowl_b200.tune --variants). All
+   variants give bit-identical results while the round-off stays below 0.5. A plan starts with its
+   shape's default. Setting a variant that is not built for the plan's H fails with OWL_ERR_ARG.
+   Drops the plan's cached squaring graphs; like the split form, set it before building batches
+   (plans of one shape and variant share a grouped launch). */
+#define OWL_COL_AUTO 0u
+#define OWL_COL_V16 1u
+#define OWL_COL_V8 2u
+#define OWL_COL_V16_OCC2 3u
+int owl_plan_set_column_variant(owl_plan* plan, uint32_t variant);
+int owl_plan_column_variant(const owl_plan* plan, uint32_t* variant);
+/* 1 if the variant (not OWL_COL_AUTO) is built for columns of H points, else 0 */
+int owl_column_variant_supported(uint32_t H, uint32_t variant);
+
 /* Word buffers -- Buffer<int> (src/Buffer.h:16-102), AllocTrac accounting aside. */
 int owl_buf_alloc(owl_plan* plan, int32_t** buf);
 int owl_buf_free(owl_plan* plan, int32_t* buf);

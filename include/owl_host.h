@@ -31,6 +31,7 @@ typedef struct {
   int split;              /* 1 = split-precision column pass (owl_plan_set_split; H = 2048 shapes only) */
   uint32_t proof_power;   /* PRP: 0 = no proof; else save the 2^p proof residues under save_dir/<E>/proof/
                              and write save_dir/proof/<E>-<p>.proof at the end (reference -proof p) */
+  uint32_t column_variant; /* OWL_COL_* of include/owl.h for the column pass; 0 = the shape's default */
 } owl_run_opts;
 
 typedef struct {

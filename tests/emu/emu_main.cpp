@@ -9,7 +9,8 @@
 //   owl_emu chain nblocks seed          (the block-carry chain vs its serial definition; "chain ok")
 // With OWL_EMU_SPLIT=1 in the environment and H = 2048 the column pass runs the
 // split-precision kernel (k_pass2_tc) on the emulated tensor cores. With OWL_EMU_NO_ROE=1 the
-// fused line passes run the build without the round-off measurement.
+// fused line passes run the build without the round-off measurement. OWL_EMU_COL=<v> runs the
+// column pass's variant v (owl::COL_V16 / COL_V8 / COL_V16_OCC2) with its stage tables.
 // Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
 #define OWL_EMU 1
 #include <algorithm>
@@ -40,6 +41,7 @@ struct EmuPlan {
   std::vector<float> roe;
   int roePos = 0;
   bool split = false;
+  int colVariant = COL_V16;
   std::vector<C> twHtc;
   std::vector<uint8_t> tcB;
 };
@@ -92,6 +94,12 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
   a.iscaleLo = std::ldexp(1.0, -(int)(E / p.t.N));
   a.loShift = p.t.loShift;
   a.timeoutNs = 60ull * 1000000000ull;
+  if (const char* cv = std::getenv("OWL_EMU_COL")) {
+    p.colVariant = std::atoi(cv);
+    if (!col_variant_ok((int)H, p.colVariant)) { throw std::runtime_error("column variant not built for H"); }
+    p.twH = toC(col_stage_tables(H, p.colVariant));
+    a.twH = p.twH.data();
+  }
   const char* sp = std::getenv("OWL_EMU_SPLIT");
   if (sp && sp[0] == '1' && H == (uint32_t)kTcH) {
     p.split = true;
@@ -111,12 +119,21 @@ template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int
   }
   emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M>(a, F, words, slot, flags, -1); });
 }
-template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {
-  constexpr int V = p2_vpt(H);
+template <int H, int M, int CV> void p2mv(EmuPlan& p, C* F, const C* Fb, C* Fq) {
+  constexpr int V = col_vpt(CV), MB = col_minb(CV);
   constexpr int T = 2 * H / V;
   size_t sm = 2 * (size_t)p2_col_stride<H, V>() * sizeof(C);
   Args a = p.a;
-  emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M, V>(a, F, Fb, Fq, -1); });
+  emu_launch(p.t.W / 2, T, sm, [=] { k_pass2<H, kR, M, V, MB>(a, F, Fb, Fq, -1); });
+}
+template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {
+  if constexpr (col_variant_ok(H, COL_V8)) {
+    if (p.colVariant == COL_V8) { return p2mv<H, M, COL_V8>(p, F, Fb, Fq); }
+  }
+  if constexpr (col_variant_ok(H, COL_V16_OCC2)) {
+    if (p.colVariant == COL_V16_OCC2) { return p2mv<H, M, COL_V16_OCC2>(p, F, Fb, Fq); }
+  }
+  p2mv<H, M, COL_V16>(p, F, Fb, Fq);
 }
 
 template <int M> void p2m_tc(EmuPlan& p, C* F, const C* Fb, C* Fq) {

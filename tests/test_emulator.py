@@ -33,8 +33,8 @@ def emu():
     return EXE
 
 
-def run(exe, *args):
-    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1")
+def run(exe, *args, **extra_env):
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", **extra_env)
     r = subprocess.run([exe] + [str(a) for a in args], capture_output=True, text=True, timeout=900, env=env)
     assert r.returncode == 0, (r.stdout[-1000:], r.stderr[-4000:])
     lines = r.stdout.strip().split("\n")
@@ -144,3 +144,18 @@ def test_emulated_square_without_roe_matches_gmp(emu, oracle, E, W, H, n, flags)
     start = np.zeros((E - 1) // 32 + 1, dtype=np.uint32)
     start[0] = 4 if flags & 2 else 3
     assert np.array_equal(got, oracle.gmp_square(E, start, n, ll=bool(flags & 2)))
+
+
+@pytest.mark.parametrize("E,W,H,n,variant", [
+    (86243, 64, 64, 12, 2),       # 8 values a thread: plan 8 * 2 * 4
+    (1300021, 64, 640, 3, 2),     # 8 values a thread: plan 8 * 4 * 5 * 4
+    (2500009, 64, 1280, 2, 2),    # 8 values a thread: plan 8 * 8 * 5 * 4
+    (4500007, 64, 2048, 2, 2),    # 8 values a thread: plan 8 * 8 * 8 * 4
+    (5600027, 64, 2560, 2, 3),    # 16 values a thread, the two-CTA launch bounds
+])
+def test_emulated_column_variants_match_gmp(emu, oracle, E, W, H, n, variant):
+    """The column pass's tile variants (owl_plan_set_column_variant) from a random start."""
+    roe, got = run(emu, "square", E, W, H, n, 0, 5, OWL_EMU_COL=str(variant))
+    want = oracle.gmp_square(E, splitmix_words(E, 5), n)
+    assert np.array_equal(got, want)
+    assert roe < 0.1

@@ -366,6 +366,89 @@ def test_batch_grouped_launches_vs_gmp(owl, oracle, ll):
             p.close()
 
 
+# every column variant besides the default one, on a shape of each kind it is built for
+VARIANT_CASES = [
+    (86243, 64, 64, "v8"), (500009, 128, 128, "v8"), (4989349, 256, 512, "v8"), (33000001, 1024, 1024, "v8"),
+    (136181029, 2048, 2048, "v8"), (1300021, 64, 640, "v8"), (2500009, 64, 1280, "v8"),
+    (80000023, 2048, 1280, "v8"), (333000017, 4096, 2560, "v16occ2"),
+]
+
+
+@pytest.mark.parametrize("E,W,H,variant", VARIANT_CASES)
+def test_column_variants_vs_gmp(owl, oracle, E, W, H, variant):
+    """A plan on another column variant (owl_plan_set_column_variant) squares bit-exactly: GMP's
+    result, and the same digits as the default variant's plan."""
+    cv = {v: k for k, v in owl.COL_NAMES.items()}[variant]
+    assert owl.column_variant_supported(H, cv)
+    n = 12 if E < 10 ** 7 else 4
+    start = random_words(E, E ^ 0xC01)
+    got = {}
+    for v in (owl.COL_AUTO, cv):
+        with owl.Plan(E, W=W, H=H, column_variant=v) as p:
+            assert v == owl.COL_AUTO or p.column_variant == cv
+            a = p.alloc()
+            p.writeIn(a, start)
+            p.squareLoop(a, a, n)
+            got[v] = p.readOut(a)
+            assert p.readROE().max() < 0.3
+    assert np.array_equal(got[cv], got[owl.COL_AUTO])
+    assert np.array_equal(got[cv], oracle.gmp_square(E, start, n))
+
+
+def test_column_variant_rules(owl):
+    """Variants not built for the plan's H are refused, OWL_COL_AUTO restores the default, and a
+    switch drops the plan's graphs (the next block still equals the default plan's)."""
+    with owl.Plan(4989349, W=256, H=512) as p:
+        default = p.column_variant
+        assert default in (owl.COL_V16, owl.COL_V8)
+        with pytest.raises(owl.OwlError):
+            p.set_column_variant(owl.COL_V16_OCC2)
+        with pytest.raises(owl.OwlError):
+            p.set_column_variant(9)
+        assert p.column_variant == default
+        a = p.alloc()
+        p.writeIn(a, small_words(p.E, 3))
+        p.squareLoop(a, a, 20)                          # a graph of the default variant
+        p.set_column_variant(owl.COL_V8 if default == owl.COL_V16 else owl.COL_V16)
+        p.squareLoop(a, a, 20)
+        p.set_column_variant(owl.COL_AUTO)
+        assert p.column_variant == default
+        p.squareLoop(a, a, 20)
+        r1 = p.bufResidue(a)
+    with owl.Plan(4989349, W=256, H=512) as q:
+        b = q.alloc()
+        q.writeIn(b, small_words(q.E, 3))
+        q.squareLoop(b, b, 60)
+        assert q.bufResidue(b) == r1
+    assert not owl.column_variant_supported(4096, owl.COL_V8)
+    assert not owl.column_variant_supported(2560, owl.COL_V8)
+    assert owl.column_variant_supported(2560, owl.COL_V16_OCC2)
+
+
+def test_batch_groups_split_by_column_variant(owl, oracle):
+    """Plans of one shape on two column variants are squared in one batch (one grouped launch per
+    variant): each equals GMP."""
+    exps = [86243, 86249, 100003, 110503]
+    plans = [owl.Plan(E, W=64, H=64, column_variant=(owl.COL_V8 if i % 2 else owl.COL_V16))
+             for i, E in enumerate(exps)]
+    try:
+        bufs, starts = [], []
+        for p in plans:
+            b = p.alloc()
+            w = random_words(p.E, p.E ^ 0x5EED)
+            p.writeIn(b, w)
+            bufs.append(b)
+            starts.append(w)
+        with owl.Batch(plans) as batch:
+            batch.square(bufs, 25)
+            batch.sync()
+        for p, b, w in zip(plans, bufs, starts):
+            assert np.array_equal(p.readOut(b), oracle.gmp_square(p.E, w, 25)), (p.E, p.column_variant)
+    finally:
+        for p in plans:
+            p.close()
+
+
 def _pattern_words(E, N, pattern):
     """0: 3, 1: 2^E - 1, 2: every raw digit 2^(bits-1) - 1 (one carry runs through all digits),
     3: zero, 4: 2^E - 2, else random."""

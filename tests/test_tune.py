@@ -37,11 +37,24 @@ def test_tune_txt_rows(tmp_path):
     assert lines == ["  12.5       64:1:128 # 294912", "  12.5      128:1:128 # 589824"]
 
 
+def test_tune_rows_with_column_variants(tmp_path):
+    """A sweep row names its column variant after the exponent in tune.txt and as element 5 in
+    tune.json, where tuned_variant finds it (and a bits/word scan keeps it)."""
+    rows = {5 << 18: (512, 1280, 30.0, 0.003, None, 2), 1 << 21: (1024, 1024, 31.0, 0.004, None, 1)}
+    out, js = tmp_path / "tune.txt", tmp_path / "tune.json"
+    tune.write(rows, 18.0, str(out), str(js))
+    assert out.read_text().splitlines() == ["  30.0      512:5:256 # 23592960 v8",
+                                            "  31.0       1K:2:512 # 37748736 v16"]
+    assert tune.tuned_variant(5 << 18, str(js)) == 2 and tune.tuned_variant(1 << 21, str(js)) == 1
+    assert tune.tuned_variant(1 << 22, str(js)) == 0 and tune.tuned_variant(1 << 22, None) == 0
+
+
 @pytest.mark.gpu
 def test_small_sweep_and_z_target(owl):
     rows = tune.tune(14, 14, 50, verbose=False)
-    (W, H, us, roe), = rows.values()
+    (W, H, us, roe, _, cv), = rows.values()
     assert 2 * W * H == 1 << 14 and us > 0 and roe < 0.1
+    assert cv in tune.variants_for(H)
     best, (b1, z1), (b2, z2) = tune.max_bpw_z(1 << 14, W, H, 19.8, verbose=False)
     assert 31 <= z1 <= 37 or abs(z1 - 34) < 4
     assert 20 <= z2 <= 25 or abs(z2 - 22) < 4
