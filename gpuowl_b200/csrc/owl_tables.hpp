@@ -84,11 +84,14 @@ inline std::vector<HostC> col_stage_tables(uint32_t H, int variant) {
 }
 
 // The column variant a plan of shape W x H starts with: the fastest of the variants built for H as
-// measured on B200 by gpuowl_b200.tune --variants (the reference's built-in tune defaults play the
-// same part, src/TuneEntry.cpp); owl_plan_set_column_variant overrides it.
+// measured on B200 by gpuowl_b200.tune --variants (time per squaring of 1,000-squaring blocks; the
+// reference's built-in tune defaults play the same part, src/TuneEntry.cpp); owl_plan_set_column_variant
+// overrides it. 8 values a thread won at 128 x 256 (10.4 against 10.7 us), 256 x 256 (10.8-10.9
+// against 11.6-11.8) and 512 x 512 (14.1 against 14.3); two CTAs per SM at 4096 x 2560 (381.3-381.6
+// against 384.0-384.8); every other measured shape keeps 16 values a thread.
 inline int default_col_variant(uint32_t W, uint32_t H) {
-  (void)W;
-  (void)H;
+  if ((W == 128 && H == 256) || (W == 256 && H == 256) || (W == 512 && H == 512)) { return COL_V8; }
+  if (W == 4096 && H == 2560) { return COL_V16_OCC2; }
   return COL_V16;
 }
 

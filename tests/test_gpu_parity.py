@@ -366,11 +366,14 @@ def test_batch_grouped_launches_vs_gmp(owl, oracle, ll):
             p.close()
 
 
-# every column variant besides the default one, on a shape of each kind it is built for
+# every column variant besides the shape's default one, on a shape of each kind it is built for
+# (the defaults: 8 values a thread at 128 x 256, 256 x 256 and 512 x 512, two CTAs per SM at
+# 4096 x 2560, else 16 values a thread)
 VARIANT_CASES = [
     (86243, 64, 64, "v8"), (500009, 128, 128, "v8"), (4989349, 256, 512, "v8"), (33000001, 1024, 1024, "v8"),
     (136181029, 2048, 2048, "v8"), (1300021, 64, 640, "v8"), (2500009, 64, 1280, "v8"),
-    (80000023, 2048, 1280, "v8"), (333000017, 4096, 2560, "v16occ2"),
+    (80000023, 2048, 1280, "v8"), (1999993, 256, 256, "v16"), (9000011, 512, 512, "v16"),
+    (333000017, 4096, 2560, "v16"),
 ]
 
 
@@ -380,6 +383,8 @@ def test_column_variants_vs_gmp(owl, oracle, E, W, H, variant):
     result, and the same digits as the default variant's plan."""
     cv = {v: k for k, v in owl.COL_NAMES.items()}[variant]
     assert owl.column_variant_supported(H, cv)
+    with owl.Plan(E, W=W, H=H) as p:
+        assert p.column_variant != cv
     n = 12 if E < 10 ** 7 else 4
     start = random_words(E, E ^ 0xC01)
     got = {}
