@@ -563,7 +563,8 @@ def run_prp_config(args, rank, world, local):
     """PRP-3 at another configuration (PRP_CONFIGS) for E the seeded prime of its range: the same timed
     steps as the 8M line (modMul(check, data) + one graph-launched block, CUDA events on the plan's
     stream, L2 flushed between steps), res64 at every 1,000 iterations against the GMP golden table
-    and a Gerbicz check at the end."""
+    and a Gerbicz check at the end. At 20M the split-precision form runs the same steps after the
+    plain one (the line's split_tc block)."""
     import torch
     import gpuowl_b200 as owl
     from gpuowl_b200 import build
@@ -577,46 +578,80 @@ def run_prp_config(args, rank, world, local):
     N = 2 * W * H
     B = args.block
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    plan = owl.Plan(E, device=local, W=W, H=H)
-    stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", local))
-    data, check, aux = plan.alloc(), plan.alloc(), plan.alloc()
-    plan.writeIn(data, [3] + [0] * (plan.nwords - 1))
-    plan.writeIn(check, [1] + [0] * (plan.nwords - 1))
-    res, step_ms = [], []
-    prof = {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
-    blk = [0]
-
-    def step():
-        k = blk[0] * B
-        blk[0] += 1
-        plan.modMul(check, data)
-        return plan.profile_square(data, B, roe=roe_measured(k, B))
-
-    for _ in range(args.warmup):
-        step()
-        res.append("%016x" % plan.bufResidue(data))
-    roe_warm = plan.readROE()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            pr = step()
-            e1.record(stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            for k, (ms, n) in pr.items():
-                prof[k][0] += ms
-                prof[k][1] += n
-            res.append("%016x" % plan.bufResidue(data))
     import numpy as np
-    roe = np.concatenate([roe_warm, plan.readROE()])
-    plan.squareLoop(aux, check, B, mul3=True)
-    plan.modMul(check, data)
-    gerbicz_ok = plan.isEqual(check, aux)
-    plan.close()
+
+    def measure(split):
+        """Warm-up and timed steps of one form of the column pass: (step times, per-kernel sums,
+        res64 per block, round-off samples, Gerbicz result, clocks)."""
+        plan = owl.Plan(E, device=local, W=W, H=H, split=split)
+        stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", local))
+        data, check, aux = plan.alloc(), plan.alloc(), plan.alloc()
+        plan.writeIn(data, [3] + [0] * (plan.nwords - 1))
+        plan.writeIn(check, [1] + [0] * (plan.nwords - 1))
+        res, step_ms = [], []
+        prof = {"pass2": [0.0, 0], "pass1": [0.0, 0], "edge": [0.0, 0]}
+        blk = [0]
+
+        def step():
+            k = blk[0] * B
+            blk[0] += 1
+            plan.modMul(check, data)
+            return plan.profile_square(data, B, roe=roe_measured(k, B))
+
+        for _ in range(args.warmup):
+            step()
+            res.append("%016x" % plan.bufResidue(data))
+        roe_warm = plan.readROE()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                pr = step()
+                e1.record(stream)
+                e1.synchronize()
+                step_ms.append(e0.elapsed_time(e1))
+                for k, (ms, n) in pr.items():
+                    prof[k][0] += ms
+                    prof[k][1] += n
+                res.append("%016x" % plan.bufResidue(data))
+        roe = np.concatenate([roe_warm, plan.readROE()])
+        plan.squareLoop(aux, check, B, mul3=True)
+        plan.modMul(check, data)
+        gerbicz_ok = plan.isEqual(check, aux)
+        plan.close()
+        return step_ms, prof, res, roe, gerbicz_ok, clocks.summary()
+
+    step_ms, prof, res, roe, gerbicz_ok, clocks = measure(False)
+    split_line = None
+    if args.workload == "prp20m" and not args.no_split:
+        s_ms, s_prof, s_res, s_roe, s_gerbicz, s_clocks = measure(True)
+        s_n = min(len(s_res), len(g["res64"])) if g else 0
+        s_value = sum(s_ms) / (args.steps * B)
+        tc_ms = s_prof["pass2"][0] / max(s_prof["pass2"][1], 1)
+        # INT8 work of one k_pass2_tc launch at H = 2560: W/2 CTAs x 2 directions x 28 digit-plane
+        # products of a 128 x 80 (outputs) x 80 (inputs) GEMM; issued with K padded to 96
+        tc_ops = 2.0 * (W // 2) * 2 * 28 * 128 * 80 * 80
+        bf16 = measured_bf16()
+        split_line = {
+            "form": "split-precision: 40-point column stages as INT8 tcgen05 GEMMs on 7 base-256 digit planes",
+            "ms_per_iter": round(s_value, 5), "ms_per_step": round(sum(s_ms) / args.steps, 4),
+            "kernel_ms": {k: round(v[0] / max(v[1], 1), 5) for k, v in s_prof.items()},
+            "max_roe": round(float(s_roe.max()), 5) if s_roe.size else None,
+            "res64_match_golden": (s_res[:s_n] == g["res64"][:s_n]) if g else None, "res64_checked": s_n,
+            "gerbicz_ok": bool(s_gerbicz),
+            "tensor_roofline": {"bound": "tensor", "kernel": "k_pass2_tc",
+                                "achieved": round(tc_ops / (tc_ms * 1e-3) / 1e12, 2),
+                                "peak": round(2 * bf16[0], 1), "unit": "TOP/s (int8)",
+                                "frac": round(tc_ops / (tc_ms * 1e-3) / 1e12 / (2 * bf16[0]), 4),
+                                "peak_kind": "2 x %s bf16 dense (int8 dense rate is twice bf16's)" % bf16[1],
+                                "int8_ops_per_launch": tc_ops},
+            "gpu_launches": (2 * B + 8) * args.steps,
+            "clocks": s_clocks,
+            "vs_plain": round(s_value / (sum(step_ms) / (args.steps * B)), 3),
+        }
     n = min(len(res), len(g["res64"])) if g else 0
     total_ms = sum(step_ms)
     dom = "pass2" if prof["pass2"][0] >= prof["pass1"][0] else "pass1"
@@ -643,7 +678,8 @@ def run_prp_config(args, rank, world, local):
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
                      "alg_bytes_per_launch": 16 * N},
         "gpu_launches": (2 * B + 8) * args.steps,
-        "clocks": clocks.summary(),
+        "clocks": clocks,
+        "split_tc": split_line,
     }
     return line
 

@@ -120,7 +120,7 @@ struct owl_plan {
   int colVariant = owl::COL_V16;
   const C* twHv16 = nullptr;
   const C* twHv8 = nullptr;
-  // split-precision column pass (H = 2048 only): DFT digit planes and its stage tables
+  // split-precision column pass (H = 2048 or 2560): DFT digit planes and its stage tables
   bool split = false;
   const unsigned char* tcB = nullptr;
   const C* twHtc = nullptr;
@@ -167,8 +167,9 @@ template <int H, int M> void setp2attr() {
   if constexpr (owl::col_variant_ok(H, owl::COL_V16_OCC2)) { setp2attr_v<H, M, owl::COL_V16_OCC2>(); }
 }
 
-template <int M> void setp2tcattr() {
-  ck(cudaFuncSetAttribute(owl::k_pass2_tc<kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, owl::kTcSmem),
+template <int H, int M> void setp2tcattr() {
+  ck(cudaFuncSetAttribute(owl::k_pass2_tc<H, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          owl::TcCfg<H>::SMEM),
      "cudaFuncSetAttribute(pass2 split)");
 }
 
@@ -200,14 +201,21 @@ void launch_pass(owl_plan* p, bool pdl, void (*kernel)(KArgs...), dim3 grid, int
   launch_on(p->stream, pdl, kernel, grid, threads, smem, args...);
 }
 
-void p2launch_tc(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
+template <int H> void p2launch_tc_h(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
   dim3 grid(p->W / 2);
-  constexpr int T = owl::kTcH / 8;
-  auto k = (mode == owl::P2_SQUARE) ? owl::k_pass2_tc<kR, owl::P2_SQUARE>
-           : (mode == owl::P2_FWD)  ? owl::k_pass2_tc<kR, owl::P2_FWD>
-                                    : owl::k_pass2_tc<kR, owl::P2_MUL>;
-  launch_pass(p, pdl, k, grid, T, owl::kTcSmem, p->args, (const unsigned char*)p->tcB, (const C*)p->twHtc, F, Fb, Fq,
-              ts);
+  constexpr int T = H / 8;
+  auto k = (mode == owl::P2_SQUARE) ? owl::k_pass2_tc<H, kR, owl::P2_SQUARE>
+           : (mode == owl::P2_FWD)  ? owl::k_pass2_tc<H, kR, owl::P2_FWD>
+                                    : owl::k_pass2_tc<H, kR, owl::P2_MUL>;
+  launch_pass(p, pdl, k, grid, T, owl::TcCfg<H>::SMEM, p->args, (const unsigned char*)p->tcB, (const C*)p->twHtc, F,
+              Fb, Fq, ts);
+}
+void p2launch_tc(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts, bool pdl) {
+  if (p->H == 2560) {
+    p2launch_tc_h<2560>(p, mode, F, Fb, Fq, ts, pdl);
+  } else {
+    p2launch_tc_h<2048>(p, mode, F, Fb, Fq, ts, pdl);
+  }
 }
 
 template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int roeSlot, int flags, int ts, bool pdl) {
@@ -274,10 +282,14 @@ void set_attrs(uint32_t W, uint32_t H) {
     default:
       fail(OWL_ERR_ARG, "unsupported H");
   }
-  if (H == (uint32_t)owl::kTcH) {
-    setp2tcattr<owl::P2_SQUARE>();
-    setp2tcattr<owl::P2_FWD>();
-    setp2tcattr<owl::P2_MUL>();
+  if (H == 2048) {
+    setp2tcattr<2048, owl::P2_SQUARE>();
+    setp2tcattr<2048, owl::P2_FWD>();
+    setp2tcattr<2048, owl::P2_MUL>();
+  } else if (H == 2560) {
+    setp2tcattr<2560, owl::P2_SQUARE>();
+    setp2tcattr<2560, owl::P2_FWD>();
+    setp2tcattr<2560, owl::P2_MUL>();
   }
 }
 
@@ -568,9 +580,12 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
 
   // tables: one allocation
   static_assert(kR == owl::kLinesPerBlock, "table layout and launch disagree on lines per block");
-  const bool tcShape = (H == (uint32_t)owl::kTcH);
-  const std::vector<owl::HostC> twHtc = tcShape ? owl::stage_tables(H, 8, owl::kTcR1) : std::vector<owl::HostC>();
-  const std::vector<uint8_t> tcB = tcShape ? owl::tc_dft_digits() : std::vector<uint8_t>();
+  const bool tcShape = owl::tc_height((int)H);
+  const std::vector<owl::HostC> twHtc =
+      H == 2048 ? owl::stage_tables(H, 8, owl::TcCfg<2048>::R1)
+                : (H == 2560 ? owl::stage_tables(H, 8, owl::TcCfg<2560>::R1) : std::vector<owl::HostC>());
+  const std::vector<uint8_t> tcB =
+      H == 2048 ? owl::tc_dft_digits<2048>() : (H == 2560 ? owl::tc_dft_digits<2560>() : std::vector<uint8_t>());
   const std::vector<owl::HostC> twH8 =
       owl::col_variant_ok((int)H, owl::COL_V8) ? owl::col_stage_tables(H, owl::COL_V8) : std::vector<owl::HostC>();
   size_t nC = t.twW.size() + t.twH.size() + twH8.size() + t.rootH.size() + t.twLo.size() + t.twHi.size() +
@@ -831,8 +846,8 @@ int owl_plan_set_timeout(owl_plan* plan, uint64_t ns) {
 int owl_plan_set_split(owl_plan* plan, int enable) {
   return guarded([&] {
     check_plan(plan);
-    if (enable && plan->H != (uint32_t)owl::kTcH) {
-      fail(OWL_ERR_ARG, "the split-precision column pass needs H = 2048");
+    if (enable && !owl::tc_height((int)plan->H)) {
+      fail(OWL_ERR_ARG, "the split-precision column pass needs H = 2048 or 2560");
     }
     DeviceGuard dg(plan->device);
     ck(cudaStreamSynchronize(plan->stream), "cudaStreamSynchronize");

@@ -7,7 +7,7 @@
 //   owl_emu modmul E W H mul3 seedA seedB
 //   owl_emu pack E N pattern            (device expand / compact vs owl_words.hpp; prints "pack ok")
 //   owl_emu chain nblocks seed          (the block-carry chain vs its serial definition; "chain ok")
-// With OWL_EMU_SPLIT=1 in the environment and H = 2048 the column pass runs the
+// With OWL_EMU_SPLIT=1 in the environment and H = 2048 or 2560 the column pass runs the
 // split-precision kernel (k_pass2_tc) on the emulated tensor cores. With OWL_EMU_NO_ROE=1 the
 // fused line passes run the build without the round-off measurement. OWL_EMU_COL=<v> runs the
 // column pass's variant v (owl::COL_V16 / COL_V8 / COL_V16_OCC2) with its stage tables.
@@ -101,10 +101,10 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
     a.twH = p.twH.data();
   }
   const char* sp = std::getenv("OWL_EMU_SPLIT");
-  if (sp && sp[0] == '1' && H == (uint32_t)kTcH) {
+  if (sp && sp[0] == '1' && tc_height((int)H)) {
     p.split = true;
-    p.twHtc = toC(stage_tables(H, 8, kTcR1));
-    p.tcB = tc_dft_digits();
+    p.twHtc = toC(stage_tables(H, 8, H == 2048 ? TcCfg<2048>::R1 : TcCfg<2560>::R1));
+    p.tcB = H == 2048 ? tc_dft_digits<2048>() : tc_dft_digits<2560>();
   }
 }
 
@@ -136,11 +136,18 @@ template <int H, int M> void p2m(EmuPlan& p, C* F, const C* Fb, C* Fq) {
   p2mv<H, M, COL_V16>(p, F, Fb, Fq);
 }
 
-template <int M> void p2m_tc(EmuPlan& p, C* F, const C* Fb, C* Fq) {
+template <int H, int M> void p2m_tch(EmuPlan& p, C* F, const C* Fb, C* Fq) {
   Args a = p.a;
   const unsigned char* tcB = p.tcB.data();
   const C* twT = p.twHtc.data();
-  emu_launch(p.t.W / 2, kTcH / 8, kTcSmem, [=] { k_pass2_tc<kR, M>(a, tcB, twT, F, Fb, Fq, -1); });
+  emu_launch(p.t.W / 2, H / 8, TcCfg<H>::SMEM, [=] { k_pass2_tc<H, kR, M>(a, tcB, twT, F, Fb, Fq, -1); });
+}
+template <int M> void p2m_tc(EmuPlan& p, C* F, const C* Fb, C* Fq) {
+  if (p.t.H == 2560) {
+    p2m_tch<2560, M>(p, F, Fb, Fq);
+  } else {
+    p2m_tch<2048, M>(p, F, Fb, Fq);
+  }
 }
 
 template <int W> void p1w(EmuPlan& p, int mode, C* F, int32_t* words, int flags) {

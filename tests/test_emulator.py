@@ -96,10 +96,12 @@ def test_emulated_radix5_random_start(emu, oracle, E, W, H, n, seed):
     assert 0 < roe < 0.1
 
 
+@pytest.mark.parametrize("E,W,H", [(4700021, 64, 2048), (5600027, 64, 2560)])
 @pytest.mark.parametrize("mode", ["square", "modmul"])
-def test_emulated_split_precision_column_pass(emu, oracle, mode):
-    """k_pass2_tc on the emulated tensor cores (descriptor decoding, digit planes, accumulators)."""
-    E, W, H = 4700021, 64, 2048
+def test_emulated_split_precision_column_pass(emu, oracle, mode, E, W, H):
+    """k_pass2_tc on the emulated tensor cores (descriptor decoding, digit planes, accumulators):
+    the 32-point GEMM stage of 2048-point columns and the 40-point one of 2560-point columns (K
+    padded to 96 bytes in two panels, outputs in chunks of 32, 32 and 16 values)."""
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", OWL_EMU_SPLIT="1")
     args = ["square", E, W, H, 2, 0, 7] if mode == "square" else ["modmul", E, W, H, 1, 11, 22]
     r = subprocess.run([emu] + [str(a) for a in args], capture_output=True, text=True, timeout=900, env=env)

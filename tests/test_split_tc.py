@@ -1,5 +1,6 @@
 """GPU parity of the split-precision column pass (owl_plan_set_split: INT8 tensor-core GEMMs on
-base-256 digit planes for the 32-point column stages) against the GMP oracle and the plain FP64 form.
+base-256 digit planes for the 32-point column stages of H = 2048 and the 40-point ones of H = 2560)
+against the GMP oracle and the plain FP64 form.
 
 Bar: bit-exact words / res64, and a round-off that stays close to the plain form's (the split form
 adds about 2^-51 relative error per GEMM output; max ROE at most 2x plain + 0.02 and below 0.35).
@@ -28,7 +29,24 @@ def test_split_square_vs_gmp(owl, oracle, E, W, H, ll):
     assert np.array_equal(got, oracle.gmp_square(E, start, n, ll=ll))
 
 
-@pytest.mark.parametrize("E,W,H", [SPLIT_SHAPES[0], SPLIT_SHAPES[2]])
+# H = 2560 shapes (40-point GEMM stage): 640K, 5M and the 20M configuration's shape
+SPLIT_SHAPES_2560 = [(5600027, 64, 2560), (90000049, 1024, 2560), (333000017, 4096, 2560)]
+
+
+@pytest.mark.parametrize("E,W,H", SPLIT_SHAPES_2560)
+@pytest.mark.parametrize("ll", [False, True])
+def test_split_2560_square_vs_gmp(owl, oracle, E, W, H, ll):
+    n = 20 if E < 10 ** 7 else 3
+    with owl.Plan(E, W=W, H=H, split=True) as p:
+        start = random_words(E, E * 5 + 1)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.squareLoop(a, a, n, ll=ll)
+        got = p.readOut(a)
+    assert np.array_equal(got, oracle.gmp_square(E, start, n, ll=ll))
+
+
+@pytest.mark.parametrize("E,W,H", [SPLIT_SHAPES[0], SPLIT_SHAPES[2], SPLIT_SHAPES_2560[0]])
 @pytest.mark.parametrize("mul3", [False, True])
 def test_split_modmul_vs_gmp(owl, oracle, E, W, H, mul3):
     with owl.Plan(E, W=W, H=H, split=True) as p:
@@ -47,6 +65,24 @@ def test_split_blocks_match_plain_and_roe(owl):
     out = {}
     for split in (False, True):
         with owl.Plan(E, W=2048, H=2048, split=split) as p:
+            a = p.alloc()
+            p.writeIn(a, small_words(E, 3))
+            p.readROE()
+            p.squareLoop(a, a, n)
+            out[split] = (p.readOut(a), float(p.readROE().max()))
+    assert np.array_equal(out[False][0], out[True][0])
+    roe_plain, roe_split = out[False][1], out[True][1]
+    assert roe_split < 0.35
+    assert roe_split <= 2 * roe_plain + 0.02, (roe_plain, roe_split)
+
+
+def test_split_blocks_match_plain_at_20m(owl):
+    """1,000 graph-launched squarings at the 20M shape (4096 x 2560) from 3: identical words in both
+    forms; ROE close."""
+    E, n = 331480451, 1000
+    out = {}
+    for split in (False, True):
+        with owl.Plan(E, W=4096, H=2560, split=split) as p:
             a = p.alloc()
             p.writeIn(a, small_words(E, 3))
             p.readROE()
