@@ -255,7 +255,8 @@ class Plan:
 
     def set_split(self, enable=True):
         """Split-precision column pass: INT8 tensor-core GEMMs for the first forward and last
-        inverse 32-point stages of every column FFT (H = 2048 only)."""
+        inverse stages of every column FFT (32-point at H = 2048, 40-point at H = 2560; other
+        heights raise OwlError)."""
         _check(self.lib.owl_plan_set_split(self.h, 1 if enable else 0))
         self.split = bool(enable)
 

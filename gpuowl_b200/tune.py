@@ -135,7 +135,7 @@ def profile_shapes(shapes, iters, bpw=16.0, device=0, split=False, variants=Fals
     """Per-kernel device time of `iters` squarings on each W x H shape (the -time profile per shape),
     and the time per squaring of a whole block (block_us): E is the first odd number above N * bpw,
     the residue random; one untimed block first. With
-    `split` the column pass runs in the split-precision form (H = 2048 only); with `variants` every
+    `split` the column pass runs in the split-precision form (H = 2048 or 2560); with `variants` every
     column variant built for H is timed, else the shape's default. The res64 after the timed block
     is returned with each row (the same for every variant of a shape)."""
     import numpy as np

@@ -78,10 +78,10 @@ int owl_plan_set_timeout(owl_plan* plan, uint64_t ns);
 /* Split-precision form of the column pass (the reference has only FP64 kernels; this selects
    between two implementations of its tailSquare / fftMiddleIn / fftMiddleOut step,
    src/cl/tailsquare.cl:225-313): with enable != 0 the first forward and last inverse
-   32-point stages of every column FFT run as INT8 tensor-core GEMMs on 7 base-256 digit
-   planes of the FP64 operands (Ozaki-style), recombined exactly in FP64. Results stay bit-exact
-   while the round-off stays below 0.5 (owl_read_roe reports it). H must be 2048 (OWL_ERR_ARG
-   otherwise). Drops the plan's cached squaring graphs; a batch keeps the form its plans had when
+   stages of every column FFT (32-point at H = 2048, 40-point at H = 2560) run as INT8
+   tensor-core GEMMs on 7 base-256 digit planes of the FP64 operands (Ozaki-style), recombined
+   exactly in FP64. Results stay bit-exact while the round-off stays below 0.5 (owl_read_roe
+   reports it). H must be 2048 or 2560 (OWL_ERR_ARG otherwise). Drops the plan's cached squaring graphs; a batch keeps the form its plans had when
    it first ran a block of that size, so set the form before building batches. */
 int owl_plan_set_split(owl_plan* plan, int enable);
 
