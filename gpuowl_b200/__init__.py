@@ -25,6 +25,8 @@ SQ_NO_ROE = 4
 # column-pass tile variants (include/owl.h OWL_COL_*)
 COL_AUTO, COL_V16, COL_V8, COL_V16_OCC2 = 0, 1, 2, 3
 COL_NAMES = {COL_V16: "v16", COL_V8: "v8", COL_V16_OCC2: "v16occ2"}
+# split-precision form flags (include/owl.h OWL_SPLIT_*)
+SPLIT_COLUMNS, SPLIT_LINES = 1, 2
 
 
 def column_variant_supported(H, variant):
@@ -212,9 +214,9 @@ class Plan:
         _check(self.lib.owl_plan_shape(self.h, ctypes.byref(N), ctypes.byref(Wv), ctypes.byref(Hv)))
         self.N, self.W, self.H = N.value, Wv.value, Hv.value
         self.nwords = n_words(self.E)
-        self.split = False
+        self.split = 0
         if split:
-            self.set_split(True)
+            self.set_split(split)
         if column_variant != COL_AUTO:
             self.set_column_variant(column_variant)
 
@@ -253,12 +255,13 @@ class Plan:
     def set_timeout(self, ns):
         _check(self.lib.owl_plan_set_timeout(self.h, int(ns)))
 
-    def set_split(self, enable=True):
-        """Split-precision column pass: INT8 tensor-core GEMMs for the first forward and last
-        inverse stages of every column FFT (32-point at H = 2048, 40-point at H = 2560; other
-        heights raise OwlError)."""
-        _check(self.lib.owl_plan_set_split(self.h, 1 if enable else 0))
-        self.split = bool(enable)
+    def set_split(self, flags=True):
+        """Split-precision form: INT8 tensor-core GEMMs for the first and last stages of every
+        column FFT (SPLIT_COLUMNS; 32-point at H = 2048, 40-point at H = 2560) and / or of every
+        line FFT (SPLIT_LINES; 16-point at W = 2048). True means SPLIT_COLUMNS; a flag whose pass
+        has no split form at this shape raises OwlError."""
+        _check(self.lib.owl_plan_set_split(self.h, int(flags)))
+        self.split = int(flags)
 
     def set_column_variant(self, variant):
         """Column-pass tile variant: COL_V16, COL_V8, COL_V16_OCC2, or COL_AUTO for the shape's
@@ -363,7 +366,7 @@ def _run(fn_name, E, device, block, log_step, check_step, stop_after, save_dir, 
     n = ctypes.c_uint32(0)
     o = RunOpts(block, log_step, check_step, stop_after, n_savefiles, W, H,
                 save_dir.encode() if save_dir else None, inject_fault_k, 1 if verbose else 0, cap,
-                ks, rs, ctypes.pointer(n), 1 if split else 0, int(proof_power), int(column_variant))
+                ks, rs, ctypes.pointer(n), int(split), int(proof_power), int(column_variant))
     r = RunResult()
     _check(getattr(lib, fn_name)(device, E, ctypes.byref(o), ctypes.byref(r)))
     return {"is_prime": bool(r.is_prime), "finished": bool(r.finished), "k": r.k, "res64": r.res64,
@@ -413,7 +416,7 @@ def worktodo_get(dir, instance=0, master_dir=None):
 def task_run(task, dir, instance=0, device=0, proof_power=0, block=1000, W=0, H=0, split=False):
     """Runs one task (reference Task::execute); returns its result JSON line (also appended to
     <dir>/results-<instance>.txt)."""
-    o = RunOpts(block, 0, 0, 0, 4, W, H, None, 0, 0, 0, None, None, None, 1 if split else 0, int(proof_power))
+    o = RunOpts(block, 0, 0, 0, 4, W, H, None, 0, 0, 0, None, None, None, int(split), int(proof_power))
     buf = ctypes.create_string_buffer(8192)
     _check(load().owl_task_run(device, str(dir).encode(), instance, ctypes.byref(task), ctypes.byref(o), buf,
                                len(buf)))

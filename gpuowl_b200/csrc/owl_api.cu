@@ -120,8 +120,9 @@ struct owl_plan {
   int colVariant = owl::COL_V16;
   const C* twHv16 = nullptr;
   const C* twHv8 = nullptr;
-  // split-precision column pass (H = 2048 or 2560): DFT digit planes and its stage tables
-  bool split = false;
+  // split-precision form: the column pass's (H = 2048 or 2560) DFT digit planes and stage tables; the
+  // line pass's (W = 2048) digit planes are args.tc1B
+  uint32_t split = 0;  // OWL_SPLIT_* flags
   const unsigned char* tcB = nullptr;
   const C* twHtc = nullptr;
   // device-side expand / compact: word staging (nWords + 1, zero padded), block carries, status
@@ -137,6 +138,15 @@ namespace {
 
 template <int W, int M> void setp1attr() {
   size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
+  if constexpr (W == owl::kLtcW) {
+    const int smx = (int)sm + owl::ltc_extra_smem();
+    ck(cudaFuncSetAttribute(owl::k_pass1<W, kR, M, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx),
+       "cudaFuncSetAttribute(pass1 split)");
+    if (M == owl::P1_FUSED) {
+      ck(cudaFuncSetAttribute(owl::k_pass1<W, kR, M, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smx),
+         "cudaFuncSetAttribute(pass1 split without round-off)");
+    }
+  }
   ck(cudaFuncSetAttribute(owl::k_pass1<W, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
      "cudaFuncSetAttribute(pass1)");
   ck(cudaFuncSetAttribute(owl::k_pass1_group<W, kR, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm),
@@ -222,6 +232,17 @@ template <int W> void p1launch(owl_plan* p, int mode, C* F, int32_t* words, int 
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * owl::p1_line_stride<W, kR>() * sizeof(C);
   dim3 grid(p->H / kR);
+  if constexpr (W == owl::kLtcW) {
+    if (p->split & OWL_SPLIT_LINES) {
+      // the split-precision line pass (its GEMM stages on the tensor cores)
+      auto k = (mode == owl::P1_FUSED) ? (roeSlot >= 0 ? owl::k_pass1<W, kR, owl::P1_FUSED, true, true>
+                                                       : owl::k_pass1<W, kR, owl::P1_FUSED, false, true>)
+               : (mode == owl::P1_IN)  ? owl::k_pass1<W, kR, owl::P1_IN, true, true>
+                                       : owl::k_pass1<W, kR, owl::P1_OUT, true, true>;
+      launch_pass(p, pdl, k, grid, T, sm + owl::ltc_extra_smem(), p->args, F, words, roeSlot, flags, ts);
+      return;
+    }
+  }
   // a fused pass with no round-off slot runs the build without the measurement
   auto k = (mode == owl::P1_FUSED) ? (roeSlot >= 0 ? owl::k_pass1<W, kR, owl::P1_FUSED>
                                                    : owl::k_pass1<W, kR, owl::P1_FUSED, false>)
@@ -321,7 +342,7 @@ void pass1(owl_plan* p, int mode, C* F, int32_t* words, int flags, int fixedSlot
 }
 
 void pass2(owl_plan* p, int mode, C* F, const C* Fb, C* Fq, int ts = -1, bool pdl = false) {
-  if (p->split) {
+  if (p->split & OWL_SPLIT_COLUMNS) {
     p2launch_tc(p, mode, F, Fb, Fq, ts, pdl);
     ck(cudaGetLastError(), "pass2 split launch");
     return;
@@ -366,7 +387,7 @@ void enqueue_square(owl_plan* p, int32_t* out, const int32_t* in, uint32_t n, ui
   }
   // the passes after the entry pass are programmatic dependents of the pass before them, except
   // the line pass after the split-precision column pass (8 us slower per iteration at 8M that way)
-  const bool pdl = !p->split;
+  const bool pdl = !(p->split & OWL_SPLIT_COLUMNS);
   pass1(p, owl::P1_IN, p->F1, const_cast<int32_t*>(in), 0, -1, ts());
   for (uint32_t k = 0; k < n; ++k) {
     pass2(p, owl::P2_SQUARE, p->F1, nullptr, nullptr, ts(), true);
@@ -586,12 +607,13 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
                 : (H == 2560 ? owl::stage_tables(H, 8, owl::TcCfg<2560>::R1) : std::vector<owl::HostC>());
   const std::vector<uint8_t> tcB =
       H == 2048 ? owl::tc_dft_digits<2048>() : (H == 2560 ? owl::tc_dft_digits<2560>() : std::vector<uint8_t>());
+  const std::vector<uint8_t> tc1B = W == (uint32_t)owl::kLtcW ? owl::line_tc_dft_digits() : std::vector<uint8_t>();
   const std::vector<owl::HostC> twH8 =
       owl::col_variant_ok((int)H, owl::COL_V8) ? owl::col_stage_tables(H, owl::COL_V8) : std::vector<owl::HostC>();
   size_t nC = t.twW.size() + t.twH.size() + twH8.size() + t.rootH.size() + t.twLo.size() + t.twHi.size() +
               twHtc.size();
-  size_t bytes = 256 * 18 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
-                 (t.x1.size() + t.x2.size() + t.p1masks.size()) * sizeof(uint32_t) + tcB.size();
+  size_t bytes = 256 * 20 + nC * sizeof(C) + (t.wt1.size() * 2 + t.wt2.size() * 2) * sizeof(double) +
+                 (t.x1.size() + t.x2.size() + t.p1masks.size()) * sizeof(uint32_t) + tcB.size() + tc1B.size();
   ck(cudaMalloc(&p->tableMem, bytes), "cudaMalloc(tables)");
   std::vector<char> host(bytes, 0);
   char* hcur = host.data();
@@ -619,6 +641,7 @@ void plan_create(int device, uint32_t E, uint32_t W, uint32_t H, owl_plan** out)
     p->twHtc = reinterpret_cast<const C*>(dbase + put(twHtc.data(), twHtc.size() * sizeof(C)));
     p->tcB = reinterpret_cast<const unsigned char*>(dbase + put(tcB.data(), tcB.size()));
   }
+  if (!tc1B.empty()) { p->args.tc1B = reinterpret_cast<const unsigned char*>(dbase + put(tc1B.data(), tc1B.size())); }
   ck(cudaMemcpy(p->tableMem, host.data(), bytes, cudaMemcpyHostToDevice), "upload tables");
 
   // FFT work buffers
@@ -843,17 +866,22 @@ int owl_plan_set_timeout(owl_plan* plan, uint64_t ns) {
   });
 }
 
-int owl_plan_set_split(owl_plan* plan, int enable) {
+int owl_plan_set_split(owl_plan* plan, int flags) {
   return guarded([&] {
     check_plan(plan);
-    if (enable && !owl::tc_height((int)plan->H)) {
+    const uint32_t f = (uint32_t)flags;
+    if (f & ~(OWL_SPLIT_COLUMNS | OWL_SPLIT_LINES)) { fail(OWL_ERR_ARG, "unknown split flags"); }
+    if ((f & OWL_SPLIT_COLUMNS) && !owl::tc_height((int)plan->H)) {
       fail(OWL_ERR_ARG, "the split-precision column pass needs H = 2048 or 2560");
+    }
+    if ((f & OWL_SPLIT_LINES) && plan->W != (uint32_t)owl::kLtcW) {
+      fail(OWL_ERR_ARG, "the split-precision line pass needs W = 2048");
     }
     DeviceGuard dg(plan->device);
     ck(cudaStreamSynchronize(plan->stream), "cudaStreamSynchronize");
     for (auto& g : plan->graphs) { cudaGraphExecDestroy(g.exec); }
     plan->graphs.clear();
-    plan->split = enable != 0;
+    plan->split = f;
   });
 }
 

@@ -66,9 +66,15 @@ struct Args {
   uint32_t eModN;      // E % N (a word is big iff its extra < E % N)
   uint32_t loShift;
   unsigned long long timeoutNs;
+  const unsigned char* tc1B;  // the split line pass's 16-point DFT digit planes (W = 2048), else null
 };
 
 enum : int { P1_FUSED = 0, P1_IN = 1, P1_OUT = 2 };
+
+}  // namespace owl
+#include "owl_tc.cuh"
+#include "owl_line_tc.cuh"
+namespace owl {
 
 // smem strides: room for the largest padding used (one pad per 2^PS elements,
 // PS >= 2), rounded so that consecutive lines start 4 elements apart mod 8
@@ -215,7 +221,9 @@ __device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
 // ROE: measure the round-off |x - rint(x)| into roe[roeSlot]. The reference measures it on a
 // sample of iterations only, with a separate kernel build (kCarryFusedROE vs kCarryFused,
 // src/Gpu.cpp:592-596); the fused line pass without it runs about 0.8 us faster at 8M.
-template <int W, int R, int MODE, bool ROE = true>
+// SPLIT (W = 2048 only): the first inverse and last forward radix-16 stages as INT8 tensor-core
+// GEMMs (owl_line_tc.cuh), the split-precision form of the line pass.
+template <int W, int R, int MODE, bool ROE = true, bool SPLIT = false>
 __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
     k_pass1(Args a, C* __restrict__ F, int32_t* __restrict__ words, int roeSlot, int flags, int tslot) {
   const uint32_t blk = blockIdx.x;
@@ -248,6 +256,7 @@ struct GroupArgs {
 template <int W, int R, int MODE, bool ROE = true>
 __global__ void __launch_bounds__(R * W / 16, occ_blocks(R * W / 16))
     k_pass1_group(const __grid_constant__ GroupArgs ga, int roeSlot, int flags) {
+  constexpr bool SPLIT = false;
   const Args& a = ga.a[blockIdx.y];
   C* __restrict__ F = ga.F[blockIdx.y];
   int32_t* __restrict__ words = ga.words[blockIdx.y];

@@ -329,7 +329,7 @@ class HostGpu {
  public:
   HostGpu(int device, uint32_t E, uint32_t W, uint32_t H, int split = 0, uint32_t colVariant = 0) : E_(E) {
     ck(owl_plan_create(device, E, W, H, &plan_));
-    if (split) { ck(owl_plan_set_split(plan_, 1)); }
+    if (split) { ck(owl_plan_set_split(plan_, split)); }
     if (colVariant) { ck(owl_plan_set_column_variant(plan_, colVariant)); }
     ck(owl_buf_alloc(plan_, &data));
     ck(owl_buf_alloc(plan_, &check));

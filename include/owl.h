@@ -75,15 +75,22 @@ int owl_plan_destroy(owl_plan* plan);
 int owl_plan_shape(const owl_plan* plan, uint32_t* N, uint32_t* W, uint32_t* H);
 /* limit of every device-side wait, in nanoseconds (default 2 s) */
 int owl_plan_set_timeout(owl_plan* plan, uint64_t ns);
-/* Split-precision form of the column pass (the reference has only FP64 kernels; this selects
-   between two implementations of its tailSquare / fftMiddleIn / fftMiddleOut step,
-   src/cl/tailsquare.cl:225-313): with enable != 0 the first forward and last inverse
-   stages of every column FFT (32-point at H = 2048, 40-point at H = 2560) run as INT8
-   tensor-core GEMMs on 7 base-256 digit planes of the FP64 operands (Ozaki-style), recombined
-   exactly in FP64. Results stay bit-exact while the round-off stays below 0.5 (owl_read_roe
-   reports it). H must be 2048 or 2560 (OWL_ERR_ARG otherwise). Drops the plan's cached squaring graphs; a batch keeps the form its plans had when
-   it first ran a block of that size, so set the form before building batches. */
-int owl_plan_set_split(owl_plan* plan, int enable);
+/* Split-precision form (the reference has only FP64 kernels; this selects between two
+   implementations of its tailSquare / fftMiddleIn / fftMiddleOut step, src/cl/tailsquare.cl:225-313,
+   and of the width FFT in carryFused, src/cl/carryfused.cl:21-231). flags:
+     OWL_SPLIT_COLUMNS  the first forward and last inverse stages of every column FFT (32-point at
+                        H = 2048, 40-point at H = 2560)
+     OWL_SPLIT_LINES    the first inverse and last forward stages of every line FFT (16-point at
+                        W = 2048)
+   run as INT8 tensor-core GEMMs on 7 base-256 digit planes of the FP64 operands (Ozaki-style),
+   recombined exactly in FP64; 0 returns to the FP64 form. Results stay bit-exact while the
+   round-off stays below 0.5 (owl_read_roe reports it). A flag whose pass has no split form at the
+   plan's shape fails with OWL_ERR_ARG. Drops the plan's cached squaring graphs; a batch keeps the
+   form its plans had when it first ran a block of that size, so set the form before building
+   batches. */
+#define OWL_SPLIT_COLUMNS 1u
+#define OWL_SPLIT_LINES 2u
+int owl_plan_set_split(owl_plan* plan, int flags);
 
 /* Column-pass tile variant -- the reference's tune.txt carries, besides the FFT shape, the build
    options measured fastest for it (src/tune.cpp:106-186, src/TuneEntry.cpp:94-105); here the choice

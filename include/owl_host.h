@@ -28,7 +28,7 @@ typedef struct {
   uint32_t* res_k;        /* iteration of each logged res64 */
   uint64_t* res_res64;    /* data res64 at that iteration */
   uint32_t* res_n;        /* number of checkpoints written */
-  int split;              /* 1 = split-precision column pass (owl_plan_set_split; H = 2048 shapes only) */
+  int split;              /* OWL_SPLIT_* flags of include/owl.h (owl_plan_set_split); 0 = FP64 form */
   uint32_t proof_power;   /* PRP: 0 = no proof; else save the 2^p proof residues under save_dir/<E>/proof/
                              and write save_dir/proof/<E>-<p>.proof at the end (reference -proof p) */
   uint32_t column_variant; /* OWL_COL_* of include/owl.h for the column pass; 0 = the shape's default */

@@ -7,9 +7,10 @@
 //   owl_emu modmul E W H mul3 seedA seedB
 //   owl_emu pack E N pattern            (device expand / compact vs owl_words.hpp; prints "pack ok")
 //   owl_emu chain nblocks seed          (the block-carry chain vs its serial definition; "chain ok")
-// With OWL_EMU_SPLIT=1 in the environment and H = 2048 or 2560 the column pass runs the
-// split-precision kernel (k_pass2_tc) on the emulated tensor cores. With OWL_EMU_NO_ROE=1 the
-// fused line passes run the build without the round-off measurement. OWL_EMU_COL=<v> runs the
+// With OWL_EMU_SPLIT=<flags> in the environment the column pass (flag 1, H = 2048 or 2560) and the
+// line pass (flag 2, W = 2048) run their split-precision kernels (k_pass2_tc, k_pass1<..., SPLIT>) on the emulated
+// tensor cores. With OWL_EMU_NO_ROE=1 the fused line passes run the build without the round-off
+// measurement. OWL_EMU_COL=<v> runs the
 // column pass's variant v (owl::COL_V16 / COL_V8 / COL_V16_OCC2) with its stage tables.
 // Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
 #define OWL_EMU 1
@@ -41,6 +42,8 @@ struct EmuPlan {
   std::vector<float> roe;
   int roePos = 0;
   bool split = false;
+  bool splitLine = false;
+  std::vector<uint8_t> tc1B;
   int colVariant = COL_V16;
   std::vector<C> twHtc;
   std::vector<uint8_t> tcB;
@@ -101,10 +104,16 @@ void init(EmuPlan& p, uint32_t E, uint32_t W, uint32_t H) {
     a.twH = p.twH.data();
   }
   const char* sp = std::getenv("OWL_EMU_SPLIT");
-  if (sp && sp[0] == '1' && tc_height((int)H)) {
+  const int spf = sp ? std::atoi(sp) : 0;  // split flags: 1 columns, 2 lines
+  if ((spf & 1) && tc_height((int)H)) {
     p.split = true;
     p.twHtc = toC(stage_tables(H, 8, H == 2048 ? TcCfg<2048>::R1 : TcCfg<2560>::R1));
     p.tcB = H == 2048 ? tc_dft_digits<2048>() : tc_dft_digits<2560>();
+  }
+  if ((spf & 2) && W == (uint32_t)kLtcW) {
+    p.splitLine = true;
+    p.tc1B = line_tc_dft_digits();
+    a.tc1B = p.tc1B.data();
   }
 }
 
@@ -112,6 +121,17 @@ template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int
   constexpr int T = kR * W / 16;
   size_t sm = (size_t)kR * p1_line_stride<W, kR>() * sizeof(C);
   Args a = p.a;
+  if constexpr (W == kLtcW) {
+    if (p.splitLine) {
+      const size_t smx = sm + ltc_extra_smem();
+      if (M == P1_FUSED && std::getenv("OWL_EMU_NO_ROE")) {
+        emu_launch(p.t.H / kR, T, smx, [=] { k_pass1<W, kR, M, false, true>(a, F, words, -1, flags, -1); });
+      } else {
+        emu_launch(p.t.H / kR, T, smx, [=] { k_pass1<W, kR, M, true, true>(a, F, words, slot, flags, -1); });
+      }
+      return;
+    }
+  }
   if (M == P1_FUSED && std::getenv("OWL_EMU_NO_ROE")) {
     // the build without the round-off measurement (OWL_SQ_NO_ROE)
     emu_launch(p.t.H / kR, T, sm, [=] { k_pass1<W, kR, M, false>(a, F, words, -1, flags, -1); });

@@ -96,13 +96,14 @@ def test_emulated_radix5_random_start(emu, oracle, E, W, H, n, seed):
     assert 0 < roe < 0.1
 
 
-@pytest.mark.parametrize("E,W,H", [(4700021, 64, 2048), (5600027, 64, 2560)])
+@pytest.mark.parametrize("E,W,H", [(4700021, 64, 2048), (5600027, 64, 2560), (4500007, 2048, 64)])
 @pytest.mark.parametrize("mode", ["square", "modmul"])
 def test_emulated_split_precision_column_pass(emu, oracle, mode, E, W, H):
-    """k_pass2_tc on the emulated tensor cores (descriptor decoding, digit planes, accumulators):
-    the 32-point GEMM stage of 2048-point columns and the 40-point one of 2560-point columns (K
-    padded to 96 bytes in two panels, outputs in chunks of 32, 32 and 16 values)."""
-    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", OWL_EMU_SPLIT="1")
+    """The split-precision passes on the emulated tensor cores (descriptor decoding, digit planes,
+    accumulators): the 32-point GEMM stage of 2048-point columns, the 40-point one of 2560-point
+    columns (K padded to 96 bytes in two panels, outputs in chunks of 32, 32 and 16 values), and the
+    16-point one of 2048-point lines (the line pass's, two M = 128 tiles, no-swizzle operands)."""
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", OWL_EMU_SPLIT="3")
     args = ["square", E, W, H, 2, 0, 7] if mode == "square" else ["modmul", E, W, H, 1, 11, 22]
     r = subprocess.run([emu] + [str(a) for a in args], capture_output=True, text=True, timeout=900, env=env)
     assert r.returncode == 0, (r.stdout[-1000:], r.stderr[-4000:])

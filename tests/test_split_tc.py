@@ -1,6 +1,6 @@
-"""GPU parity of the split-precision column pass (owl_plan_set_split: INT8 tensor-core GEMMs on
-base-256 digit planes for the 32-point column stages of H = 2048 and the 40-point ones of H = 2560)
-against the GMP oracle and the plain FP64 form.
+"""GPU parity of the split-precision form (owl_plan_set_split: INT8 tensor-core GEMMs on base-256
+digit planes for the 32-point column stages of H = 2048, the 40-point ones of H = 2560 and the
+16-point line stages of W = 2048) against the GMP oracle and the plain FP64 form.
 
 Bar: bit-exact words / res64, and a round-off that stays close to the plain form's (the split form
 adds about 2^-51 relative error per GEMM output; max ROE at most 2x plain + 0.02 and below 0.35).
@@ -12,8 +12,10 @@ from conftest import random_words, small_words
 
 pytestmark = pytest.mark.gpu
 
-# H = 2048 shapes: 256K, 2M and the 8M wavefront shape
+# H = 2048 shapes: 256K, 2M and the 8M wavefront shape (whose 2048-point lines are split too)
 SPLIT_SHAPES = [(4700021, 64, 2048), (37000003, 512, 2048), (136181029, 2048, 2048)]
+# W = 2048 shapes whose columns have no split form: the line pass alone on the tensor cores
+SPLIT_LINE_SHAPES = [(4500007, 2048, 64), (80000023, 2048, 1280)]
 
 
 @pytest.mark.parametrize("E,W,H", SPLIT_SHAPES)
@@ -46,10 +48,24 @@ def test_split_2560_square_vs_gmp(owl, oracle, E, W, H, ll):
     assert np.array_equal(got, oracle.gmp_square(E, start, n, ll=ll))
 
 
-@pytest.mark.parametrize("E,W,H", [SPLIT_SHAPES[0], SPLIT_SHAPES[2], SPLIT_SHAPES_2560[0]])
+@pytest.mark.parametrize("E,W,H", SPLIT_LINE_SHAPES)
+@pytest.mark.parametrize("ll", [False, True])
+def test_split_line_pass_vs_gmp(owl, oracle, E, W, H, ll):
+    """The line pass's 16-point GEMM stages (W = 2048) with FP64 columns, against GMP."""
+    n = 20 if E < 10 ** 7 else 4
+    with owl.Plan(E, W=W, H=H, split=owl.SPLIT_LINES) as p:
+        start = random_words(E, E * 11 + 3)
+        a = p.alloc()
+        p.writeIn(a, start)
+        p.squareLoop(a, a, n, ll=ll)
+        got = p.readOut(a)
+    assert np.array_equal(got, oracle.gmp_square(E, start, n, ll=ll))
+
+
+@pytest.mark.parametrize("E,W,H", [SPLIT_SHAPES[0], SPLIT_SHAPES[2], SPLIT_SHAPES_2560[0], SPLIT_LINE_SHAPES[0]])
 @pytest.mark.parametrize("mul3", [False, True])
 def test_split_modmul_vs_gmp(owl, oracle, E, W, H, mul3):
-    with owl.Plan(E, W=W, H=H, split=True) as p:
+    with owl.Plan(E, W=W, H=H, split=all_split(owl, W, H)) as p:
         wa, wb = random_words(E, 15), random_words(E, 16)
         a, b = p.alloc(), p.alloc()
         p.writeIn(a, wa)
@@ -74,6 +90,29 @@ def test_split_blocks_match_plain_and_roe(owl):
     roe_plain, roe_split = out[False][1], out[True][1]
     assert roe_split < 0.35
     assert roe_split <= 2 * roe_plain + 0.02, (roe_plain, roe_split)
+
+
+def all_split(owl, W, H):
+    """Every split-precision pass the shape has."""
+    return (owl.SPLIT_COLUMNS if H in (2048, 2560) else 0) | (owl.SPLIT_LINES if W == 2048 else 0)
+
+
+def test_split_both_passes_at_8m_match_plain(owl):
+    """1,000 graph-launched squarings at 8M from 3 with both passes split: identical words to the
+    plain form; ROE close."""
+    E, n = 136181029, 1000
+    out = {}
+    for split in (0, owl.SPLIT_COLUMNS | owl.SPLIT_LINES):
+        with owl.Plan(E, W=2048, H=2048, split=split) as p:
+            assert p.split == split
+            a = p.alloc()
+            p.writeIn(a, small_words(E, 3))
+            p.readROE()
+            p.squareLoop(a, a, n)
+            out[split] = (p.readOut(a), float(p.readROE().max()))
+    (w0, r0), (w1, r1) = out.values()
+    assert np.array_equal(w0, w1)
+    assert r1 < 0.35 and r1 <= 2 * r0 + 0.02, (r0, r1)
 
 
 def test_split_blocks_match_plain_at_20m(owl):
@@ -105,10 +144,16 @@ def test_split_prp_driver_gerbicz(owl):
 
 
 def test_split_rejects_other_heights(owl):
+    """A split flag whose pass has no split form at the plan's shape is refused."""
     with owl.Plan(1000003, W=128, H=256) as p:
-        with pytest.raises(owl.OwlError) as e:
-            p.set_split(True)
-        assert e.value.status == -1
+        for flags in (True, owl.SPLIT_LINES, 4):
+            with pytest.raises(owl.OwlError) as e:
+                p.set_split(flags)
+            assert e.value.status == -1
+    with owl.Plan(4500007, W=2048, H=64) as p:
+        with pytest.raises(owl.OwlError):
+            p.set_split(owl.SPLIT_COLUMNS)
+        p.set_split(owl.SPLIT_LINES)
 
 
 def test_tc_wait_timeout_probe_keeps_plan_usable(owl, oracle):
