@@ -135,7 +135,8 @@ def profile_shapes(shapes, iters, bpw=16.0, device=0, split=False, variants=Fals
     """Per-kernel device time of `iters` squarings on each W x H shape (the -time profile per shape),
     and the time per squaring of a whole block (block_us): E is the first odd number above N * bpw,
     the residue random; one untimed block first. With
-    `split` the column pass runs in the split-precision form (H = 2048 or 2560); with `variants` every
+    `split` (OWL_SPLIT_* flags) the column pass (H = 2048 or 2560) and / or the line pass (W = 2048)
+    run in the split-precision form; with `variants` every
     column variant built for H is timed, else the shape's default. The res64 after the timed block
     is returned with each row (the same for every variant of a shape)."""
     import numpy as np
@@ -418,7 +419,8 @@ def main():
     ap.add_argument("--criterion", default="z", choices=["z", "roe"],
                     help="with --bpw-scan: round-off Z = 28 (the reference's) or max round-off < --roe-limit")
     ap.add_argument("--shapes", metavar="WxH,...", help="per-pass times of these shapes (at 16 bits/word)")
-    ap.add_argument("--split", action="store_true", help="with --shapes: the split-precision column pass")
+    ap.add_argument("--split", type=int, nargs="?", const=1, default=0, metavar="FLAGS",
+                    help="with --shapes: the split-precision form (1 column pass, 2 line pass, 3 both)")
     ap.add_argument("--variants", action="store_true",
                     help="with --shapes: time every column variant built for the shape's H")
     ap.add_argument("--no-variants", action="store_true", help="sweep: the shapes' default column variants only")
