@@ -11,7 +11,8 @@
 // line pass (flag 2, W = 2048) run their split-precision kernels (k_pass2_tc, k_pass1<..., SPLIT>) on the emulated
 // tensor cores. With OWL_EMU_NO_ROE=1 the fused line passes run the build without the round-off
 // measurement. OWL_EMU_COL=<v> runs the
-// column pass's variant v (owl::COL_V16 / COL_V8 / COL_V16_OCC2) with its stage tables.
+// column pass's variant v (owl::COL_V16 / COL_V8 / COL_V16_OCC2) with its stage tables. With
+// OWL_EMU_GROUP=1 the line passes run the grouped kernel of a batch (one plan as the group).
 // Output: one line "roe <max>" then one line of nWords hex u32 (little-endian order).
 #define OWL_EMU 1
 #include <algorithm>
@@ -131,6 +132,19 @@ template <int W, int M> void p1m(EmuPlan& p, C* F, int32_t* words, int slot, int
       }
       return;
     }
+  }
+  if (std::getenv("OWL_EMU_GROUP")) {
+    // the grouped kernel of a batch, as a group of this one plan
+    GroupArgs ga{};
+    ga.a[0] = a;
+    ga.F[0] = F;
+    ga.words[0] = words;
+    if (M == P1_FUSED && std::getenv("OWL_EMU_NO_ROE")) {
+      emu_launch(p.t.H / kR, T, sm, [=] { k_pass1_group<W, kR, M, false>(ga, -1, flags); });
+    } else {
+      emu_launch(p.t.H / kR, T, sm, [=] { k_pass1_group<W, kR, M>(ga, slot, flags); });
+    }
+    return;
   }
   if (M == P1_FUSED && std::getenv("OWL_EMU_NO_ROE")) {
     // the build without the round-off measurement (OWL_SQ_NO_ROE)

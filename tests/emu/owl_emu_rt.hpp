@@ -215,7 +215,9 @@ template <typename F> void emu_launch(unsigned grid, unsigned block, size_t dynS
       Job& j = jobs[(size_t)g * block + t];
       j.f = &f;
       j.t.tid.x = t;
+      j.t.tid.y = j.t.tid.z = 0;
       j.t.bid.x = g;
+      j.t.bid.y = j.t.bid.z = 0;  // one-dimensional grids (a grouped launch of one plan)
       j.t.bdim.x = block;
       j.t.gdim.x = grid;
       j.t.cta = ctas[g].get();

@@ -162,3 +162,18 @@ def test_emulated_column_variants_match_gmp(emu, oracle, E, W, H, n, variant):
     want = oracle.gmp_square(E, splitmix_words(E, 5), n)
     assert np.array_equal(got, want)
     assert roe < 0.1
+
+
+@pytest.mark.parametrize("E,W,H,n,flags", [
+    (1300021, 64, 640, 3, 0),     # 8-thread line-group CTAs
+    (1000003, 128, 256, 6, 2),    # 16-thread CTAs, LL
+    (1999993, 256, 256, 4, 0),    # 32-thread CTAs
+])
+def test_emulated_grouped_line_pass(emu, oracle, E, W, H, n, flags):
+    """The batch's grouped line-pass kernel (k_pass1_group, here with a group of one plan) from a
+    random start."""
+    ll = bool(flags & 2)
+    roe, got = run(emu, "square", E, W, H, n, flags, 9, OWL_EMU_GROUP="1")
+    want = oracle.gmp_square(E, splitmix_words(E, 9), n, ll=ll)
+    assert np.array_equal(got, want)
+    assert roe < 0.1
