@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--block", type=int, default=BLOCK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision (tensor-core) form")
+    ap.add_argument("--batch-shapes", default="default", choices=["default", "tuned"],
+                    help="batch64: the library's W x H split per FFT size, or the split and column variant "
+                         "that gpuowl_b200/tune_b200.json holds for that size (the FFT size is the same)")
     ap.add_argument("--no-configs", action="store_true",
                     help="prp8m on one GPU: skip the short runs of the other configurations (20M, 256K, "
                          "batch64) whose lines the 8M line carries under \"configs\"")
@@ -513,9 +516,17 @@ def run_batch64(args, rank, world, local):
     torch.cuda.set_device(local)
     B = args.block
     plans, bufs = [], []
+    table = {}
+    if getattr(args, "batch_shapes", "default") == "tuned":
+        with open(os.path.join(ROOT, "gpuowl_b200", "tune_b200.json")) as f:
+            table = json.load(f)
     for E in exps:
         N, W, H = owl.fft_choose(E, 19.0)
-        p = owl.Plan(E, device=local, W=W, H=H)
+        cv = owl.COL_AUTO
+        if str(N) in table:
+            W, H = int(table[str(N)][0]), int(table[str(N)][1])
+            cv = int(table[str(N)][5]) if len(table[str(N)]) >= 6 and table[str(N)][5] else owl.COL_AUTO
+        p = owl.Plan(E, device=local, W=W, H=H, column_variant=cv)
         b = p.alloc()
         p.writeIn(b, [3] + [0] * (p.nwords - 1))
         plans.append(p)
@@ -560,6 +571,9 @@ def run_batch64(args, rank, world, local):
             "config": {"workload": "64 exponents log-uniform in [1M,20M] (seed 20261203), FFT per exponent at <=19 "
                                    "bits/word, one graph launch per %d-iteration block" % B,
                        "fft_sizes": shapes, "timing": "wall clock around launch + synchronize",
+                       "shapes": "W x H split and column variant per FFT size: %s" % (
+                           "the tuner's table (gpuowl_b200/tune_b200.json)"
+                           if getattr(args, "batch_shapes", "default") == "tuned" else "the library's defaults"),
                        "launches": "plans of one W x H shape (%d shapes) share one launch per pass: %d kernels per "
                                    "iteration for the %d plans" % (len(groups), sum(2 * ((n + 15) // 16)
                                                                                    for n in groups.values()),
