@@ -311,10 +311,11 @@ def test_batch64_golden(owl):
             p.close()
 
 
-def test_batch64_long_golden(owl):
-    """The 12 smallest exponents of the batch (64K and 80K FFTs: plans of one shape run as grouped
-    launches) for 10,000 iterations: res64 at every 1,000 equal the GMP golden table."""
-    golden = load_golden("batch64_long")
+def test_batch64_10k_golden(owl):
+    """All 64 exponents of the batch (9 FFT sizes from 64K to 1M, plans of one shape as grouped
+    launches) for 10,000 iterations in one batch: res64 at every 1,000 equal the GMP golden table
+    (640 checkpoints)."""
+    golden = load_golden("batch64_10k")
     plans = []
     for it in golden["items"]:
         _, W, H = owl.fft_choose(it["E"], 19.0)
