@@ -153,9 +153,10 @@ def measured_bf16():
     return 1590.0, "fallback"
 
 
-def profiled_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "traffic_8m.json")
+def profiled_traffic(name="8m"):
+    """Per-launch DRAM bytes of the pass kernels from the committed ncu summary
+    (profiles/traffic_<name>.json), if any."""
+    path = os.path.join(ROOT, "profiles", "traffic_%s.json" % name)
     if os.path.exists(path):
         with open(path) as f:
             return json.load(f)
@@ -717,7 +718,8 @@ def run_prp_config(args, rank, world, local):
         "kernel_ms": {k: round(v[0] / max(v[1], 1), 5) for k, v in prof.items()},
         "roofline": {"bound": "hbm", "kernel": "k_pass2" if dom == "pass2" else "k_pass1",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": profiled_traffic(args.workload[3:]).get(dom),
                      "alg_bytes_per_launch": 16 * N},
         "gpu_launches": (2 * B + 8) * args.steps,
         "clocks": clocks,
