@@ -179,10 +179,10 @@ def fft_choose(E, max_bpw=0.0, tune=None):
         with open(tune) as f:
             t = json.load(f)
         # with measured max bits/word (tune --bpw-scan): the smallest FFT whose limit covers E
-        # (or max_bpw when given)
+        # (or max_bpw when given) and that holds at least 8 bits per word (the engine's lower bound)
         scanned = sorted((int(n), v) for n, v in t.items() if len(v) >= 5 and v[4])
         for n, v in scanned:
-            if E / n <= (max_bpw if max_bpw > 0 else v[4]):
+            if 8 <= E / n <= (max_bpw if max_bpw > 0 else v[4]):
                 return n, int(v[0]), int(v[1])
         if str(N.value) in t:
             return N.value, int(t[str(N.value)][0]), int(t[str(N.value)][1])
@@ -413,10 +413,11 @@ def worktodo_get(dir, instance=0, master_dir=None):
     return t if found.value else None
 
 
-def task_run(task, dir, instance=0, device=0, proof_power=0, block=1000, W=0, H=0, split=False):
+def task_run(task, dir, instance=0, device=0, proof_power=0, block=1000, W=0, H=0, split=False, column_variant=0):
     """Runs one task (reference Task::execute); returns its result JSON line (also appended to
     <dir>/results-<instance>.txt)."""
-    o = RunOpts(block, 0, 0, 0, 4, W, H, None, 0, 0, 0, None, None, None, int(split), int(proof_power))
+    o = RunOpts(block, 0, 0, 0, 4, W, H, None, 0, 0, 0, None, None, None, int(split), int(proof_power),
+                int(column_variant))
     buf = ctypes.create_string_buffer(8192)
     _check(load().owl_task_run(device, str(dir).encode(), instance, ctypes.byref(task), ctypes.byref(o), buf,
                                len(buf)))

@@ -111,3 +111,7 @@ def test_fft_choose_with_measured_bpw_table(lib, tmp_path):
     assert g.fft_choose(150000001, tune=str(p)) == (1 << 23, 2048, 2048)     # 17.9 bits/word
     assert g.fft_choose(152000001, tune=str(p)) == (1 << 24, 4096, 2048)     # 18.1 > 18.0 at 8M
     assert g.fft_choose(333000017, tune=str(p)) == (5 << 22, 4096, 2560)     # 19.8 at 16M, 15.9 at 20M
+    # an exponent below 8 bits/word of every measured size falls back to the library's size and
+    # takes that size's tuned split: M86243 on the 8K FFT of the committed table
+    committed = os.path.join(ROOT, "gpuowl_b200", "tune_b200.json")
+    assert g.fft_choose(86243, tune=committed) == (8192, 64, 64)
