@@ -597,7 +597,7 @@ def run_batch64(args, rank, world, local):
 PRP_CONFIGS = {
     "prp20m": ("prp_20m", 4096, 2560, "20M (5*2^22)", "[330M,335M]",
                "proof power 8 configured (its first residue point, at E/256, lies beyond the timed "
-               "iterations; tests/test_large.py runs the driver with it)"),
+               "iterations; tests/test_large.py runs the PRP driver with it)"),
     "prp256k": ("prp_256k", 0, 0, "256K", "[4.8M,5.0M]", ""),
 }
 
