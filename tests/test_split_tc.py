@@ -8,7 +8,7 @@ adds about 2^-51 relative error per GEMM output; max ROE at most 2x plain + 0.02
 import numpy as np
 import pytest
 
-from conftest import random_words, small_words
+from conftest import load_golden, random_words, small_words
 
 pytestmark = pytest.mark.gpu
 
@@ -191,3 +191,16 @@ def test_split_plans_in_one_batch(owl, oracle):
     finally:
         for p in plans:
             p.close()
+
+
+@pytest.mark.parametrize("name,W,H,flags", [("prp_8m", 2048, 2048, 3), ("prp_20m", 4096, 2560, 1)])
+def test_split_prp_driver_golden(owl, name, W, H, flags):
+    """The PRP driver (Gerbicz check every block) in the split-precision form at the 8M (both passes
+    split) and 20M (column pass split) configurations: res64 at every 1,000 iterations equal to the
+    GMP golden table, no check failure."""
+    g = load_golden(name)
+    r = owl.prp_run(g["E"], W=W, H=H, block=1000, log_step=1000, stop_after=g["iters"], split=flags)
+    assert r["n_errors"] == 0 and r["k"] >= g["iters"]
+    got = {k: "%016x" % v for k, v in r["checkpoints"]}
+    for i, want in enumerate(g["res64"]):
+        assert got.get((i + 1) * g["step"]) == want, (i + 1) * g["step"]
