@@ -545,6 +545,7 @@ void sync_and_check(owl_plan* p) {
     uint32_t G = p->H / kR;
     ck(cudaMemset(p->args.ctl, 0, sizeof(owl::Ctl)), "reset ctl");
     ck(cudaMemset(p->args.flags, 0, G * sizeof(uint32_t)), "reset flags");
+    ck(cudaMemset(p->args.shuttle, 0, (size_t)G * p->W * sizeof(long long)), "reset carry words");
     fail(OWL_ERR_TIMEOUT, "device-side carry wait timed out");
   }
 }

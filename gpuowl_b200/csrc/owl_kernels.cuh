@@ -54,7 +54,7 @@ struct Args {
   const uint32_t* x2;  // per (line j2, e): X2 = step*(2 j2 + e) mod N
   const uint2* p1masks; // per (line group g, pass-1 thread t): the big-word and wrap bits of the thread's
                         // 32 words, bit (r R + ll) 2 + e for column t + (W/RL) r, line g R + ll, word e
-  long long* shuttle;  // carry rows, (H/R) x W
+  long long* shuttle;  // carry words, (H/R) x W; 0 = consumed, else the carry encoded (kCarryOffset)
   long long* pending;  // (word index, carry) pairs, kPendingCap entries
   uint32_t* flags;     // per line group
   Ctl* ctl;
@@ -115,6 +115,8 @@ __device__ __forceinline__ long long sext_low(long long x, uint32_t bits) {
 }
 
 constexpr double RNDVAL = 3.0 * 2251799813685248.0;  // 3 * 2^51
+// offset of an integer carry word in the carry rows (words are never 0: 0 marks a consumed word)
+constexpr long long kCarryOffset = 1ll << 62;
 
 // launch timestamps for the profiler: slot < 0 turns them off
 __device__ __forceinline__ void ts_begin(const Args& a, int slot) {
@@ -226,6 +228,7 @@ __device__ __forceinline__ C one_mul(C a, C b, C c, C d, C t2) {
 template <int W, int R, int MODE, bool ROE = true, bool SPLIT = false>
 __global__ void __launch_bounds__(R * W / 16, (R * W / 16 == 256) ? 2 : 1)
     k_pass1(Args a, C* __restrict__ F, int32_t* __restrict__ words, int roeSlot, int flags, int tslot) {
+  constexpr bool REGBOUND = false;
   const uint32_t blk = blockIdx.x;
 #include "owl_pass1_body.inc"
 }
@@ -257,6 +260,7 @@ template <int W, int R, int MODE, bool ROE = true>
 __global__ void __launch_bounds__(R * W / 16, occ_blocks(R * W / 16))
     k_pass1_group(const __grid_constant__ GroupArgs ga, int roeSlot, int flags) {
   constexpr bool SPLIT = false;
+  constexpr bool REGBOUND = true;
   const Args& a = ga.a[blockIdx.y];
   C* __restrict__ F = ga.F[blockIdx.y];
   int32_t* __restrict__ words = ga.words[blockIdx.y];

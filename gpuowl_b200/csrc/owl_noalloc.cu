@@ -169,6 +169,8 @@ __global__ void k_noalloc_tables(owl::Args a, uint32_t twWn, uint32_t twHn) {
     }
   }
   for (uint32_t i = tid; i < H / kR; i += nth) { a.flags[i] = 0; }
+  // carry words: 0 = consumed (a call that stopped on an error may have left some set)
+  for (uint32_t i = tid; i < (H / kR) * W; i += nth) { a.shuttle[i] = 0; }
   if (tid == 0) {
     a.ctl->ticket = 0;
     a.ctl->error = 0;

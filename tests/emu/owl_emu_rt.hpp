@@ -171,6 +171,10 @@ inline uint32_t ld_acquire(const uint32_t* p) {
   return std::atomic_ref<uint32_t>(*const_cast<uint32_t*>(p)).load(std::memory_order_acquire);
 }
 inline void st_release(uint32_t* p, uint32_t v) { std::atomic_ref<uint32_t>(*p).store(v, std::memory_order_release); }
+inline long long ld_relaxed(const long long* p) {
+  return std::atomic_ref<long long>(*const_cast<long long*>(p)).load(std::memory_order_relaxed);
+}
+inline void st_relaxed(long long* p, long long v) { std::atomic_ref<long long>(*p).store(v, std::memory_order_relaxed); }
 inline unsigned long long gtimer() {
   return (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
              std::chrono::steady_clock::now().time_since_epoch())
