@@ -177,3 +177,17 @@ def test_emulated_grouped_line_pass(emu, oracle, E, W, H, n, flags):
     want = oracle.gmp_square(E, splitmix_words(E, 9), n, ll=ll)
     assert np.array_equal(got, want)
     assert roe < 0.1
+
+
+@pytest.mark.parametrize("E,W,H,n,flags", [
+    (1999993, 1024, 64, 6, 0),    # 128-thread CTAs: all carry words requested at once, then polled
+    (4500007, 2048, 64, 4, 2),    # 256-thread CTAs: carry words polled one after another, LL
+])
+def test_emulated_self_publishing_carry_words(emu, oracle, E, W, H, n, flags):
+    """The line passes from W = 1024 up publish their carry rows word by word (never-0 encoded
+    words, each consumer thread polling and clearing its own) instead of with a flag."""
+    ll = bool(flags & 2)
+    roe, got = run(emu, "square", E, W, H, n, flags, 13)
+    want = oracle.gmp_square(E, splitmix_words(E, 13), n, ll=ll)
+    assert np.array_equal(got, want)
+    assert roe < 0.1
